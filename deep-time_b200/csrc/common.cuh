@@ -1,0 +1,141 @@
+// Shared helpers of the deep-time B200 backend: status handling, complex arithmetic on CUDA's
+// vector types, and the deterministic block reductions every CG kernel uses.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <type_traits>
+
+#include "deeptime_gpu.h"
+
+namespace dt {
+
+// The message behind the last non-OK status of this thread (dt_last_error).
+void set_error(const char* fmt, ...);
+const char* last_error();
+
+#define DT_CUDA(call)                                                                        \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) {                                                                 \
+      ::dt::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));   \
+      return e_ == cudaErrorMemoryAllocation ? DT_OOM : DT_DEVICE_ERROR;                     \
+    }                                                                                        \
+  } while (0)
+
+#define DT_TRY(expr)             \
+  do {                           \
+    dt_status s_ = (expr);       \
+    if (s_ != DT_OK) return s_;  \
+  } while (0)
+
+template <class T>
+struct cx;
+template <>
+struct cx<double> {
+  using type = double2;
+};
+template <>
+struct cx<float> {
+  using type = float2;
+};
+template <class T>
+using cplx = typename cx<T>::type;
+
+template <class C>
+__host__ __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
+  C r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <class C>
+__device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <class C>
+__device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <class C>
+__device__ __forceinline__ C cmul(C a, C b) { return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <class C>
+__device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+template <class C>
+__device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
+// i * a
+template <class C>
+__device__ __forceinline__ C cmuli(C a) { return mk<C>(-a.y, a.x); }
+
+// ---- deterministic reductions -------------------------------------------------------------
+// A reducing kernel writes one partial per block (fixed grid, fixed in-block order); the last
+// block to finish (an atomic ticket) sums the partials in index order. The result therefore does
+// not depend on the order blocks ran in.
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Sum over the block (any multiple of 32 threads up to 1024); the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v, double* scratch32) {
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  lane = tid & 31;
+  warp = tid >> 5;
+  v = warp_sum(v);
+  __syncthreads();
+  if (lane == 0) scratch32[warp] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (warp == 0) {
+    r = lane < nwarps ? scratch32[lane] : 0.0;
+    r = warp_sum(r);
+  }
+  return r;
+}
+__device__ __forceinline__ double block_max(double v, double* scratch32) {
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  int lane = tid & 31, warp = tid >> 5;
+  int nwarps = (blockDim.x * blockDim.y + 31) >> 5;
+  v = warp_max(v);
+  __syncthreads();
+  if (lane == 0) scratch32[warp] = v;
+  __syncthreads();
+  double r = -INFINITY;
+  if (warp == 0) {
+    r = lane < nwarps ? scratch32[lane] : -INFINITY;
+    r = warp_max(r);
+  }
+  return r;
+}
+
+// After thread 0 of each block stored its partial(s), returns true in thread 0 of exactly one
+// block: the last to arrive, which then sees every partial. `ticket` is reset for reuse.
+__device__ __forceinline__ bool last_block(unsigned int* ticket, unsigned int nblocks) {
+  __shared__ bool is_last;
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  if (tid == 0) {
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    is_last = (t == nblocks - 1);
+    if (is_last) *ticket = 0u;
+  }
+  __syncthreads();
+  return is_last;
+}
+
+inline unsigned int ceil_div(size_t a, size_t b) { return (unsigned int)((a + b - 1) / b); }
+inline bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }
+inline int ilog2(long v) {
+  int r = 0;
+  while ((1L << r) < v) ++r;
+  return r;
+}
+
+}  // namespace dt

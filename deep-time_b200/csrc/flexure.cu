@@ -1,0 +1,1472 @@
+// Lithospheric flexure on the B200: (L D L + C) x = b by preconditioned conjugate gradients.
+//
+// This is the device implementation behind dt_flex_* (include/deeptime_gpu.h). It solves the
+// system of the reference's flexure::Solver (crates/deeptime-core/src/surface/flexure.rs:
+// operator :1546-1624, Spectral :1108-1348, Bank :1352-1402, Preconditioner :1405-1468,
+// Solver::solve :1680-1740) with its own kernels:
+//
+//   k_apply      the 13-point variable-D biharmonic y = L(d L v) + c v over a shared-memory tile
+//                with a 2-cell halo (x wraps, rows clamp), fused with the CG reduction of its
+//                caller (p.Ap, ||b - Ax||^2, or the Jacobi sandwich of the preconditioner);
+//   k_rows_fwd   per row: a real FFT of length w as a complex FFT of length w/2 (even samples
+//                real, odd imaginary) and the usual split, written in a packed half spectrum:
+//                column 0 holds (X[0], X[w/2]), both real;
+//   k_cols       per group of columns: the DCT-II along y by Makhoul's reordering and one complex
+//                FFT of length h, the division by d lambda^2 + c, the inverse DCT, all in shared
+//                memory: one read and one write of the half spectrum;
+//   k_rows_inv   the inverse of k_rows_fwd, fused with what its caller needs next (store, weighted
+//                accumulation for the bank's blend, or r.z and max|z|);
+//   k_update, k_direction  the CG vector updates with their reductions.
+//
+// Reductions are deterministic: per-block partials in a fixed grid and a fixed order, summed by
+// the last block to finish. The PCG loop runs on the device as a CUDA-graph conditional WHILE
+// node: the last kernels of an iteration decide whether the body runs again, so a solve makes no
+// host round trip per iteration.
+//
+// Precision: the kernels are templated on T (double or float). DT_PREC_FP64 runs everything in
+// double; DT_PREC_MIXED runs the inner PCG in float on a scaled residual and refines in double
+// (residual b - A x, the solution and every dot-product accumulator stay double).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "fft.cuh"
+
+namespace dt {
+
+// ---------------------------------------------------------------------------------------------
+// Device-resident solver state. One per precision lane; kernels read and update it.
+
+enum { SITE_PAP = 0, SITE_UPDATE = 1, SITE_PRECOND = 2, SITE_RESID = 3, SITE_STATS = 4, SITE_DOT = 5, SITE_MISC = 6 };
+enum { STOP_RUNNING = 0, STOP_CONVERGED = 1, STOP_BREAKDOWN = 2, STOP_CAP = 3, STOP_NONFINITE = 4 };
+
+struct Scalars {
+  // problem
+  double bb;      // ||b||^2 of the system being solved
+  double tol;     // MAX_Z: metres; REL: relative residual
+  int max_it;
+  int rule;       // DT_STOP_*
+  int n;
+  // iteration
+  double rz, pap, alpha, beta, rr, err, rz_new;
+  int it;
+  int stop;
+  int started;    // the first preconditioning (before the loop) is done
+  int body_runs;
+  // preconditioner bank (flexure.rs:1352-1402)
+  double lo, hi, sum_c, sum_d;
+  double node_d[3];
+  double c_ref;
+  int levels;
+  // misc reductions
+  double dot_out, max_out;
+  unsigned long long cond;  // graph conditional handle, 0 outside a graph
+  unsigned int ticket[8];
+};
+
+__device__ __forceinline__ void set_cond(Scalars* S, unsigned int v) {
+  if (S->cond) cudaGraphSetConditional((cudaGraphConditionalHandle)S->cond, v);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Last-block finishers: the scalar work between kernels.
+
+__device__ void finish_pap(Scalars* S, double pap) {
+  S->pap = pap;
+  if (!(isfinite(pap) && pap > 0.0)) {
+    S->stop = isfinite(pap) ? STOP_BREAKDOWN : STOP_NONFINITE;
+    set_cond(S, 0);
+    return;
+  }
+  S->alpha = S->rz / pap;
+}
+
+__device__ void finish_update(Scalars* S, double rr) {
+  S->rr = rr;
+  S->it += 1;
+  if (!isfinite(rr)) {
+    S->stop = STOP_NONFINITE;
+  } else if (S->rule == DT_STOP_REL_RESIDUAL && rr <= S->tol * S->tol * S->bb) {
+    S->stop = STOP_CONVERGED;
+  } else if (S->rule == DT_STOP_RMS_RESIDUAL && rr <= S->tol * S->tol * (double)S->n) {
+    S->stop = STOP_CONVERGED;
+  } else if (S->rule != DT_STOP_MAX_Z && S->it >= S->max_it) {
+    S->stop = STOP_CAP;
+  }
+  if (S->stop) set_cond(S, 0);
+}
+
+// After z = M^-1 r: rz = r.z, err = max|z| (flexure.rs:1719-1737).
+__device__ void finish_precond(Scalars* S, double rz, double err) {
+  S->err = err;
+  S->rz_new = rz;
+  if (!isfinite(rz) || !isfinite(err)) {
+    S->stop = STOP_NONFINITE;
+    set_cond(S, 0);
+    return;
+  }
+  if (!S->started) {
+    S->started = 1;
+    S->rz = rz;
+    if (S->rule == DT_STOP_MAX_Z && err < S->tol) S->stop = STOP_CONVERGED;
+    return;
+  }
+  if (S->rule == DT_STOP_MAX_Z) {
+    if (err < S->tol) {
+      S->stop = STOP_CONVERGED;
+    } else if (S->it >= S->max_it) {
+      S->stop = STOP_CAP;
+    }
+  }
+  if (S->stop) {
+    set_cond(S, 0);
+    return;
+  }
+  S->beta = rz / S->rz;
+  S->rz = rz;
+}
+
+// Bank::new from ln(alpha) extremes and the sums (flexure.rs:1361-1401); `mean_d` selects the
+// single mean level instead.
+__device__ void finish_stats(Scalars* S, double lo, double hi, double sum_c, double sum_d, double dx, bool mean_d) {
+  const double RHO_MANTLE = 3300.0;
+  double n = (double)max(S->n, 1);
+  S->lo = lo;
+  S->hi = hi;
+  S->sum_c = sum_c;
+  S->sum_d = sum_d;
+  S->c_ref = sum_c / n;
+  if (mean_d) {
+    S->levels = 1;
+    S->node_d[0] = sum_d / n;
+    return;
+  }
+  auto node_d = [&](double ln_a) {
+    double a = exp(ln_a) * dx;
+    double a2 = a * a;
+    return RHO_MANTLE * (a2 * a2) / 4.0;
+  };
+  double floor_ = log(0.4);
+  if (hi - lo < 0.05 || hi <= floor_) {
+    S->levels = 1;
+    S->node_d[0] = node_d(0.5 * (lo + hi));
+    return;
+  }
+  lo = fmax(lo, floor_);
+  S->lo = lo;
+  S->levels = 3;
+  for (int k = 0; k < 3; ++k) S->node_d[k] = node_d(lo + (hi - lo) * (double)k / 2.0);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Reduction epilogue shared by the kernels: block partials -> last block -> finisher.
+
+template <int NV>
+struct Acc {
+  double v[NV];
+};
+
+// Writes this block's partial sums (thread 0 holds them) and, in the last block, reduces all of
+// them in index order. kind: 0 sum, 1 max (per component).
+template <int NV>
+__device__ bool reduce_partials(Acc<NV>& a, const int* kind, double* partials, unsigned int* ticket, unsigned int nblocks) {
+  __shared__ double scratch[32];
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  int nthreads = blockDim.x * blockDim.y;
+  unsigned int bid = blockIdx.x + blockIdx.y * gridDim.x;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double r = kind[q] ? block_max(a.v[q], scratch) : block_sum(a.v[q], scratch);
+    if (tid == 0) partials[(size_t)q * nblocks + bid] = r;
+  }
+  if (!last_block(ticket, nblocks)) return false;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = kind[q] ? -INFINITY : 0.0;
+    for (unsigned int b = tid; b < nblocks; b += nthreads) {
+      double p = __ldcg(partials + (size_t)q * nblocks + b);
+      s = kind[q] ? fmax(s, p) : s + p;
+    }
+    double r = kind[q] ? block_max(s, scratch) : block_sum(s, scratch);
+    a.v[q] = r;  // valid in thread 0
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------------------------
+// The 13-point operator over a tile.
+
+enum {
+  AP_DOT = 0,     // y = A v, reduce v.y                        (CG: Ap, p.Ap)
+  RESID = 1,      // y = b - A v, reduce y.y                    (refinement residual)
+  JAC_LEFT = 2,   // u = J r;         y = r - A u               (preconditioner: left)
+  JAC_FINAL = 3,  // u = J r + part;  y = u + J (r - A u), reduce r.y and max|y|
+  PLAIN = 4,      // y = A v
+  BEND = 5        // y = L (d L v)
+};
+
+constexpr int TBX = 64, TBY = 16, TTY = 4;  // tile of 64 x 16 cells, 64 x 4 threads
+
+template <class T, int MODE>
+__global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, const T* __restrict__ v, const T* __restrict__ J,
+                                                    const T* __restrict__ part, const T* __restrict__ d,
+                                                    const T* __restrict__ c, const T* __restrict__ rb, T* __restrict__ y,
+                                                    double* partials, Scalars* S) {
+  if (MODE != PLAIN && MODE != BEND && MODE != RESID) {
+    if (S->stop) {
+      if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) set_cond(S, 0);
+      return;
+    }
+  }
+  __shared__ T sv[TBY + 4][TBX + 4];
+  __shared__ T sm[TBY + 2][TBX + 2];
+  const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
+  const int tid = threadIdx.x + threadIdx.y * TBX;
+  constexpr int NT = TBX * TTY;
+  // v (or the vector the mode forms) with a 2-cell halo: rows clamp, columns wrap
+  for (int idx = tid; idx < (TBY + 4) * (TBX + 4); idx += NT) {
+    int jj = idx / (TBX + 4), ii = idx - jj * (TBX + 4);
+    int gj = min(max(j0 - 2 + jj, 0), h - 1);
+    int gi = i0 - 2 + ii;
+    gi = ((gi % w) + w) % w;
+    size_t k = (size_t)gj * w + gi;
+    T val;
+    if (MODE == JAC_LEFT) {
+      val = J[k] * rb[k];
+    } else if (MODE == JAC_FINAL) {
+      val = J[k] * rb[k] + part[k];
+    } else {
+      val = v[k];
+    }
+    sv[jj][ii] = val;
+  }
+  __syncthreads();
+  // m = d . L v on the tile plus a 1-cell halo (rows of m clamp the same way)
+  for (int idx = tid; idx < (TBY + 2) * (TBX + 2); idx += NT) {
+    int mj = idx / (TBX + 2), mi = idx - mj * (TBX + 2);
+    int gm = min(max(j0 - 1 + mj, 0), h - 1);
+    int gi = i0 - 1 + mi;
+    gi = ((gi % w) + w) % w;
+    int rn = max(gm - 1, 0) - j0 + 2, rc = gm - j0 + 2, rs = min(gm + 1, h - 1) - j0 + 2;
+    T west = sv[rc][mi], east = sv[rc][mi + 2], mid = sv[rc][mi + 1];
+    T lap = (west + east + sv[rn][mi + 1] + sv[rs][mi + 1] - (T)4 * mid) * inv_dx2;
+    sm[mj][mi] = lap * d[(size_t)gm * w + gi];
+  }
+  __syncthreads();
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  const int oi = threadIdx.x;
+  const int i = i0 + oi;
+#pragma unroll
+  for (int q = 0; q < TBY / TTY; ++q) {
+    int oj = threadIdx.y + q * TTY;
+    int j = j0 + oj;
+    if (i < w && j < h) {
+      int mn = max(j - 1, 0) - j0 + 1, mc = oj + 1, ms = min(j + 1, h - 1) - j0 + 1;
+      T lm = (sm[mc][oi] + sm[mc][oi + 2] + sm[mn][oi + 1] + sm[ms][oi + 1] - (T)4 * sm[mc][oi + 1]) * inv_dx2;
+      size_t k = (size_t)j * w + i;
+      T u = sv[oj + 2][oi + 2];
+      if (MODE == BEND) {
+        y[k] = lm;
+      } else {
+        T au = lm + c[k] * u;
+        if (MODE == AP_DOT) {
+          y[k] = au;
+          acc.v[0] += (double)u * (double)au;
+        } else if (MODE == PLAIN) {
+          y[k] = au;
+        } else if (MODE == RESID) {
+          T rr = rb[k] - au;
+          y[k] = rr;
+          acc.v[0] += (double)rr * (double)rr;
+        } else if (MODE == JAC_LEFT) {
+          y[k] = rb[k] - au;
+        } else {  // JAC_FINAL
+          T r = rb[k];
+          T z = u + J[k] * (r - au);
+          y[k] = z;
+          acc.v[0] += (double)r * (double)z;
+          acc.v[1] = fmax(acc.v[1], fabs((double)z));
+        }
+      }
+    }
+  }
+  if (MODE == AP_DOT || MODE == RESID || MODE == JAC_FINAL) {
+    const int kind[2] = {0, 1};
+    unsigned int nb = gridDim.x * gridDim.y;
+    int site = MODE == AP_DOT ? SITE_PAP : MODE == RESID ? SITE_RESID : SITE_PRECOND;
+    bool last = MODE == JAC_FINAL ? reduce_partials<2>(acc, kind, partials, &S->ticket[site], nb)
+                                  : reduce_partials<1>(*reinterpret_cast<Acc<1>*>(&acc), kind, partials, &S->ticket[site], nb);
+    if (last && tid == 0) {
+      if (MODE == AP_DOT) finish_pap(S, acc.v[0]);
+      if (MODE == RESID) S->rr = acc.v[0];
+      if (MODE == JAC_FINAL) finish_precond(S, acc.v[0], acc.v[1]);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// CG vector kernels (grid-stride).
+
+// x += alpha p; r -= alpha Ap; reduce r.r
+template <class T>
+__global__ void __launch_bounds__(256) k_update(size_t n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
+                                                const T* __restrict__ ap, double* partials, Scalars* S) {
+  if (S->stop) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(S, 0);
+    return;
+  }
+  T alpha = (T)S->alpha;
+  Acc<1> acc;
+  acc.v[0] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] += alpha * p[k];
+    T rv = r[k] - alpha * ap[k];
+    r[k] = rv;
+    acc.v[0] += (double)rv * (double)rv;
+  }
+  const int kind[1] = {0};
+  if (reduce_partials<1>(acc, kind, partials, &S->ticket[SITE_UPDATE], gridDim.x) && threadIdx.x == 0) finish_update(S, acc.v[0]);
+}
+
+// p = z + beta p; also the loop's guard: the body runs again only while nothing stopped it and
+// fewer than max_it + 2 bodies ran.
+template <class T>
+__global__ void __launch_bounds__(256) k_direction(size_t n, T* __restrict__ p, const T* __restrict__ z, Scalars* S) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int runs = ++S->body_runs;
+    bool again = S->stop == 0 && runs < S->max_it + 2;
+    if (!again && S->stop == 0) S->stop = STOP_CAP;
+    set_cond(S, again ? 1u : 0u);
+  }
+  if (S->stop) return;
+  T beta = (T)S->beta;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    p[k] = z[k] + beta * p[k];
+}
+
+template <class A, class B>
+__global__ void k_convert(size_t n, const A* __restrict__ a, B* __restrict__ b) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) b[k] = (B)a[k];
+}
+
+// r32 = r64 * s (s from the residual's RMS), e32 = 0
+__global__ void k_scale_down(size_t n, const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ e32,
+                             const Scalars* S64, double* scale_out) {
+  double s = S64->rr > 0 ? sqrt((double)n / S64->rr) : 1.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale_out = s;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    r32[k] = (float)(r[k] * s);
+    e32[k] = 0.0f;
+  }
+}
+
+// x64 += e32 / s
+__global__ void k_accumulate(size_t n, double* __restrict__ x, const float* __restrict__ e32, const double* scale) {
+  double inv = 1.0 / *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += (double)e32[k] * inv;
+}
+
+template <class T>
+__global__ void k_fill(size_t n, T* __restrict__ a, T v) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) a[k] = v;
+}
+
+// reduce a.b (and max |b| when MAXB) into S->dot_out / S->max_out
+template <class T>
+__global__ void __launch_bounds__(256) k_dot(size_t n, const T* __restrict__ a, const T* __restrict__ b, double* partials, Scalars* S,
+                                             int site) {
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    acc.v[0] += (double)a[k] * (double)b[k];
+    acc.v[1] = fmax(acc.v[1], fabs((double)b[k]));
+  }
+  const int kind[2] = {0, 1};
+  if (reduce_partials<2>(acc, kind, partials, &S->ticket[site], gridDim.x) && threadIdx.x == 0) {
+    S->dot_out = acc.v[0];
+    S->max_out = acc.v[1];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Preconditioner set-up (flexure.rs:1361-1401 and :1426-1460).
+
+template <class T>
+__global__ void __launch_bounds__(256) k_stats(size_t n, const T* __restrict__ d, const T* __restrict__ c, double dx, int mean_d,
+                                               double* partials, Scalars* S) {
+  const double RHO_MANTLE = 3300.0;
+  Acc<4> acc;
+  acc.v[0] = -INFINITY;  // -lo as a max
+  acc.v[1] = -INFINITY;  // hi
+  acc.v[2] = 0.0;        // sum c
+  acc.v[3] = 0.0;        // sum d
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    double dv = (double)d[k];
+    double la = log(pow(4.0 * fmax(dv, 1e-30) / RHO_MANTLE, 0.25) / dx);
+    acc.v[0] = fmax(acc.v[0], -la);
+    acc.v[1] = fmax(acc.v[1], la);
+    acc.v[2] += (double)c[k];
+    acc.v[3] += dv;
+  }
+  const int kind[4] = {1, 1, 0, 0};
+  if (reduce_partials<4>(acc, kind, partials, &S->ticket[SITE_STATS], gridDim.x) && threadIdx.x == 0)
+    finish_stats(S, -acc.v[0], acc.v[1], acc.v[2], acc.v[3], dx, mean_d != 0);
+}
+
+// Per cell: the bank's weights (squares sum to one) and the damped Jacobi weight 1/2 / diag.
+template <class T>
+__global__ void __launch_bounds__(256) k_bank_weights(int w, int h, const T* __restrict__ d, const T* __restrict__ c, double dx,
+                                                      T* __restrict__ w0, T* __restrict__ w1, T* __restrict__ w2,
+                                                      T* __restrict__ jac, const Scalars* S) {
+  const double RHO_MANTLE = 3300.0;
+  size_t n = (size_t)w * h;
+  double lo = S->lo, hi = S->hi;
+  double inv4 = 1.0 / (dx * dx * dx * dx);
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % w), j = (int)(k / w);
+    double dv = (double)d[k];
+    double la = log(pow(4.0 * fmax(dv, 1e-30) / RHO_MANTLE, 0.25) / dx);
+    double t = fmin(fmax((la - lo) / (hi - lo), 0.0), 1.0) * 2.0;
+    int k0 = min((int)floor(t), 1);
+    double f = t - (double)k0;
+    double a = sqrt(1.0 - f), b = sqrt(f);
+    w0[k] = (T)(k0 == 0 ? a : 0.0);
+    w1[k] = (T)(k0 == 0 ? b : a);
+    w2[k] = (T)(k0 == 1 ? b : 0.0);
+    double east = (double)d[(size_t)j * w + (i + 1) % w], west = (double)d[(size_t)j * w + (i + w - 1) % w];
+    double north = (double)d[(size_t)max(j - 1, 0) * w + i], south = (double)d[(size_t)min(j + 1, h - 1) * w + i];
+    double around = east + west + north + south;
+    jac[k] = (T)(0.5 / ((double)c[k] + (16.0 * dv + around) * inv4));
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// The spectral solve (flexure.rs:1183-1347), three passes over a packed half spectrum of h rows
+// by N = w/2 complex values.
+
+enum { INV_STORE = 0, INV_ACCUM = 1, INV_STORE_DOT = 2, INV_STORE_W = 3 };
+
+// Rows per block so that a block has at least one warp (RB * N / 8 >= 32).
+inline int rows_per_block(int N) { return std::max(1, 256 / N); }
+
+template <class T, bool WEIGHT>
+__global__ void __launch_bounds__(1024) k_rows_fwd(int w, int h, const T* __restrict__ v, const T* __restrict__ wt, cplx<T>* __restrict__ half,
+                           const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ post, const Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int N = w >> 1;
+  const int logN = __ffs(N) - 1;
+  const int RB = blockDim.x * 8 / N;
+  const int row0 = blockIdx.x * RB;
+  const int tid = threadIdx.x;
+  // load rows as complex pairs (v[2n], v[2n+1]): one 2-wide vector load per pair
+  for (int idx = tid; idx < RB * N; idx += blockDim.x) {
+    int rb = idx / N, nn = idx - rb * N;
+    int j = row0 + rb;
+    C z = mk<C>((T)0, (T)0);
+    if (j < h) {
+      size_t k = (size_t)j * w + 2 * nn;
+      z = *reinterpret_cast<const C*>(v + k);
+      if (WEIGHT) {
+        C ww = *reinterpret_cast<const C*>(wt + k);
+        z.x *= ww.x;
+        z.y *= ww.y;
+      }
+    }
+    s[idx] = z;
+  }
+  __syncthreads();
+  smem_fft<C, false>(s, N, logN, tw);
+  // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
+  for (int idx = tid; idx < RB * (N / 2 + 1); idx += blockDim.x) {
+    int rb = idx / (N / 2 + 1), kk = idx - rb * (N / 2 + 1);
+    int j = row0 + rb;
+    if (j >= h) continue;
+    C* row = s + (size_t)rb * N;
+    C* out = half + (size_t)j * N;
+    if (kk == 0) {
+      C z0 = row[0];
+      out[0] = mk<C>(z0.x + z0.y, z0.x - z0.y);  // (X[0], X[N]) both real
+      continue;
+    }
+    C zk = row[kk], zn = row[N - kk];
+    C E = mk<C>((zk.x + zn.x) * (T)0.5, (zk.y - zn.y) * (T)0.5);
+    C O = mk<C>((zk.y + zn.y) * (T)0.5, (zn.x - zk.x) * (T)0.5);
+    C wo = cmul(post[kk], O);
+    out[kk] = cadd(E, wo);
+    if (kk != N - kk) out[N - kk] = cconj(csub(E, wo));
+  }
+}
+
+// The column pass: DCT-II along y (Makhoul), divide by d lambda^2 + c_ref, inverse DCT.
+// lx[k] = 2 cos(2 pi k / w) - 2 for k = 0..N; ly[m] = 2 cos(pi m / h) - 2.
+template <class T>
+__global__ void __launch_bounds__(1024) k_cols(int N, int h, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ omega,
+                       const T* __restrict__ lx, const T* __restrict__ ly, T inv_dx2, const Scalars* S, int level) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int CPB = blockDim.x * 8 / h;
+  const int k0 = blockIdx.x * CPB;
+  const int logh = __ffs(h) - 1;
+  const int tid = threadIdx.x;
+  const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
+  // gather with the even-first / odd-reversed order
+  for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
+    int j = idx / CPB, cc = idx - j * CPB;
+    int k = k0 + cc;
+    C x = k < N ? half[(size_t)j * N + k] : mk<C>((T)0, (T)0);
+    int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
+    s[(size_t)cc * h + pos] = x;
+  }
+  __syncthreads();
+  smem_fft<C, false>(s, h, logh, tw);
+  // per column and pair (m, h - m): C[m] = (w_m V[m] + i w_(h-m) V[h-m]) / 2, divide, and back
+  for (int idx = tid; idx < CPB * (h / 2 + 1); idx += blockDim.x) {
+    int cc = idx / (h / 2 + 1), m = idx - cc * (h / 2 + 1);
+    int k = k0 + cc;
+    if (k >= N) continue;
+    C* col = s + (size_t)cc * h;
+    // divisors: column 0 is packed (real part k = 0, imaginary part k = N)
+    auto den = [&](int kx, int mm) {
+      T l = (lx[kx] + ly[mm]) * inv_dx2;
+      return dref * (l * l) + cref;
+    };
+    if (m == 0) {
+      C v0 = col[0];
+      if (k == 0) {
+        v0.x /= den(0, 0);
+        v0.y /= den(N, 0);
+      } else {
+        T dd = den(k, 0);
+        v0.x /= dd;
+        v0.y /= dd;
+      }
+      col[0] = v0;
+      continue;
+    }
+    int mm = h - m;
+    C p = cmul(omega[m], col[m]);
+    C q = cmul(omega[mm], col[mm]);
+    C cm = cscale(cadd(p, cmuli(q)), (T)0.5);
+    C cn = cscale(cadd(q, cmuli(p)), (T)0.5);
+    if (k == 0) {
+      cm.x /= den(0, m);
+      cm.y /= den(N, m);
+      cn.x /= den(0, mm);
+      cn.y /= den(N, mm);
+    } else {
+      T a = den(k, m), b = den(k, mm);
+      cm.x /= a;
+      cm.y /= a;
+      cn.x /= b;
+      cn.y /= b;
+    }
+    // V'[m] = conj(w_m) (C[m] - i C[h-m])
+    C vm = cmul(cconj(omega[m]), csub(cm, cmuli(cn)));
+    C vn = cmul(cconj(omega[mm]), csub(cn, cmuli(cm)));
+    col[m] = vm;
+    if (mm != m) col[mm] = vn;
+  }
+  __syncthreads();
+  smem_fft<C, true>(s, h, logh, tw);
+  const T inv_h = (T)1 / (T)h;
+  for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
+    int j = idx / CPB, cc = idx - j * CPB;
+    int k = k0 + cc;
+    if (k >= N) continue;
+    int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
+    half[(size_t)j * N + k] = cscale(s[(size_t)cc * h + pos], inv_h);
+  }
+}
+
+// Inverse rows: Z[k] = E[k] + i O[k] with E = (X[k] + conj X[N-k]) / 2,
+// O = (X[k] - conj X[N-k]) conj(W^k) / 2; x = IFFT_N(Z) / N de-interleaved.
+template <class T, int MODE>
+__global__ void __launch_bounds__(1024) k_rows_inv(int w, int h, const cplx<T>* __restrict__ half, T* __restrict__ out, const T* __restrict__ wt,
+                           const T* __restrict__ r, const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ post,
+                           double* partials, Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) {
+    if (MODE == INV_STORE_DOT && blockIdx.x == 0 && threadIdx.x == 0) set_cond(S, 0);
+    return;
+  }
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  const int N = w >> 1;
+  const int logN = __ffs(N) - 1;
+  const int RB = blockDim.x * 8 / N;
+  const int row0 = blockIdx.x * RB;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < RB * (N / 2 + 1); idx += blockDim.x) {
+    int rb = idx / (N / 2 + 1), kk = idx - rb * (N / 2 + 1);
+    int j = row0 + rb;
+    C* row = s + (size_t)rb * N;
+    if (j >= h) {
+      row[kk] = mk<C>((T)0, (T)0);
+      if (kk > 0 && kk < N) row[N - kk] = mk<C>((T)0, (T)0);
+      continue;
+    }
+    const C* in = half + (size_t)j * N;
+    if (kk == 0) {
+      C p = in[0];  // (X[0], X[N])
+      row[0] = mk<C>((p.x + p.y) * (T)0.5, (p.x - p.y) * (T)0.5);
+      continue;
+    }
+    C xk = in[kk], xn = in[N - kk];
+    // for index kk
+    C E = mk<C>((xk.x + xn.x) * (T)0.5, (xk.y - xn.y) * (T)0.5);
+    C D = mk<C>((xk.x - xn.x) * (T)0.5, (xk.y + xn.y) * (T)0.5);
+    C O = cmul(D, cconj(post[kk]));
+    row[kk] = cadd(E, cmuli(O));
+    if (kk != N - kk) {
+      // for index N - kk: E' = conj E, D' = -conj D, conj(W^(N-k)) = -W^k  => O' = conj(D) W^k
+      C E2 = cconj(E);
+      C O2 = cmul(cconj(D), post[kk]);
+      row[N - kk] = cadd(E2, cmuli(O2));
+    }
+  }
+  __syncthreads();
+  smem_fft<C, true>(s, N, logN, tw);
+  const T inv_n = (T)1 / (T)N;
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  for (int idx = tid; idx < RB * N; idx += blockDim.x) {
+    int rb = idx / N, nn = idx - rb * N;
+    int j = row0 + rb;
+    if (j >= h) continue;
+    size_t k = (size_t)j * w + 2 * nn;
+    C z = cscale(s[idx], inv_n);
+    C* o = reinterpret_cast<C*>(out + k);
+    if (MODE == INV_STORE) {
+      *o = z;
+    } else if (MODE == INV_STORE_W) {
+      C ww = *reinterpret_cast<const C*>(wt + k);
+      *o = mk<C>(z.x * ww.x, z.y * ww.y);
+    } else if (MODE == INV_ACCUM) {
+      C ww = *reinterpret_cast<const C*>(wt + k);
+      C prev = *o;
+      *o = mk<C>(prev.x + z.x * ww.x, prev.y + z.y * ww.y);
+    } else {  // INV_STORE_DOT
+      *o = z;
+      C rr = *reinterpret_cast<const C*>(r + k);
+      acc.v[0] += (double)rr.x * (double)z.x + (double)rr.y * (double)z.y;
+      acc.v[1] = fmax(acc.v[1], fmax(fabs((double)z.x), fabs((double)z.y)));
+    }
+  }
+  if (MODE == INV_STORE_DOT) {
+    const int kind[2] = {0, 1};
+    if (reduce_partials<2>(acc, kind, partials, &S->ticket[SITE_PRECOND], gridDim.x) && tid == 0) finish_precond(S, acc.v[0], acc.v[1]);
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Small control kernels.
+
+// Before the loop: give the scalars the graph's conditional handle and run the body only when
+// nothing has stopped the solve yet.
+__global__ void k_arm(Scalars* S, unsigned long long handle) {
+  S->cond = handle;
+  S->body_runs = 0;
+  cudaGraphSetConditional((cudaGraphConditionalHandle)handle, S->stop == 0 ? 1u : 0u);
+}
+__global__ void k_disarm(Scalars* S) { S->cond = 0ull; }
+
+// A fresh solve state (keeps the problem fields, the bank and the handle slot cleared).
+__global__ void k_reset(Scalars* S) {
+  S->it = 0;
+  S->stop = 0;
+  S->started = 0;
+  S->body_runs = 0;
+  S->err = 0.0;
+  S->cond = 0ull;
+  for (int k = 0; k < 8; ++k) S->ticket[k] = 0u;
+}
+
+// bb = dot_out (from a k_dot of b with itself)
+__global__ void k_take_bb(Scalars* S) { S->bb = S->dot_out; }
+__global__ void k_rr_is_bb(Scalars* S) { S->rr = S->bb; }
+
+// The first guess's fate: keep x0 (r = b - A x0 already formed, S->rr) when it beats x = 0,
+// i.e. ||b - A x0|| < ||b||; otherwise x = 0 and r = b.
+template <class T>
+__global__ void k_warm_decide(size_t n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ b, const Scalars* S) {
+  bool keep = S->rr < S->bb;
+  if (keep) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] = (T)0;
+    r[k] = b[k];
+  }
+}
+struct WarmInfo {
+  int accepted;
+  double rel;
+};
+__global__ void k_warm_record(Scalars* S, WarmInfo* info) {
+  info->accepted = S->rr < S->bb ? 1 : 0;
+  info->rel = S->bb > 0 ? sqrt(S->rr / S->bb) : 0.0;
+  if (!info->accepted) S->rr = S->bb;
+}
+
+// The loop's entry checks (flexure.rs:1691-1704 and the relative-residual rule).
+__global__ void k_begin(Scalars* S) {
+  S->it = 0;
+  S->stop = 0;
+  S->started = 0;
+  S->body_runs = 0;
+  S->err = 0.0;
+  if (!isfinite(S->bb) || !isfinite(S->rr)) {
+    S->stop = STOP_NONFINITE;
+  } else if (!(S->bb > 0.0)) {
+    S->stop = STOP_CONVERGED;  // b = 0: x = 0 is exact
+  } else if (S->rule != DT_STOP_MAX_Z) {
+    double lim = S->rule == DT_STOP_REL_RESIDUAL ? S->tol * S->tol * S->bb : S->tol * S->tol * (double)S->n;
+    if (S->rr <= lim) S->stop = STOP_CONVERGED;
+  }
+}
+
+// After the first preconditioning under the reference's rule: when max|z| < tol already, the
+// preconditioner's answer is the correction (flexure.rs:1699-1702).
+template <class T>
+__global__ void k_initial_result(size_t n, T* __restrict__ x, const T* __restrict__ z, const Scalars* S) {
+  if (!(S->rule == DT_STOP_MAX_Z && S->stop == STOP_CONVERGED && S->started && S->it == 0)) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += z[k];
+}
+
+// ---------------------------------------------------------------------------------------------
+// Host side.
+
+static thread_local char g_err[1024] = "";
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+const char* last_error() { return g_err; }
+
+template <class T>
+struct Tables {
+  cplx<T>* tw_row = nullptr;  // N = w/2 entries e^(-2 pi i t / N)
+  cplx<T>* post = nullptr;    // N entries e^(-2 pi i k / w)
+  cplx<T>* tw_col = nullptr;  // h entries e^(-2 pi i t / h)
+  cplx<T>* omega = nullptr;   // h entries e^(-i pi m / 2h)
+  T* lx = nullptr;            // N + 1 entries 2 cos(2 pi k / w) - 2
+  T* ly = nullptr;            // h entries 2 cos(pi m / h) - 2
+};
+
+template <class T>
+struct Lane {
+  T *d = nullptr, *c = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
+  T *J = nullptr, *wt[3] = {nullptr, nullptr, nullptr}, *left = nullptr, *part = nullptr;
+  cplx<T>* half = nullptr;
+  Tables<T> tab;
+  Scalars* S = nullptr;
+  cudaGraph_t graph[2] = {nullptr, nullptr};  // [levels == 3]
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+};
+
+static const long double PI_L = 3.14159265358979323846264338327950288L;
+
+}  // namespace dt
+
+struct dt_flex {
+  int w = 0, h = 0, N = 0;
+  double dx = 0;
+  size_t n = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  dt::Lane<double> L64;
+  dt::Lane<float> L32;
+  double* b64 = nullptr;
+  double* partials = nullptr;
+  double* scale = nullptr;  // mixed: the residual scale of the current refinement
+  dt::WarmInfo* warm = nullptr;
+  std::vector<void*> allocs;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sms = 148;
+};
+
+namespace dt {
+
+template <class T>
+static dt_status dalloc(dt_flex* s, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? DT_OOM : DT_DEVICE_ERROR;
+  }
+  s->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return DT_OK;
+}
+
+template <class T>
+static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
+  int N = s->N, h = s->h, w = s->w;
+  std::vector<cplx<T>> a(N), b(N), c(h), o(h);
+  std::vector<T> lx(N + 1), ly(h);
+  for (int t = 0; t < N; ++t) {
+    long double ang = -2.0L * PI_L * t / N;
+    a[t] = mk<cplx<T>>((T)cosl(ang), (T)sinl(ang));
+    long double ang2 = -2.0L * PI_L * t / w;
+    b[t] = mk<cplx<T>>((T)cosl(ang2), (T)sinl(ang2));
+  }
+  for (int t = 0; t < h; ++t) {
+    long double ang = -2.0L * PI_L * t / h;
+    c[t] = mk<cplx<T>>((T)cosl(ang), (T)sinl(ang));
+    long double ang2 = -PI_L * t / (2.0L * h);
+    o[t] = mk<cplx<T>>((T)cosl(ang2), (T)sinl(ang2));
+  }
+  // the Laplacian's symbols as the reference forms them (flexure.rs:1145-1150), in double
+  for (int k = 0; k <= N; ++k) lx[k] = (T)(2.0 * std::cos(6.283185307179586476925286766559 * (double)k / (double)w) - 2.0);
+  for (int m = 0; m < h; ++m) ly[m] = (T)(2.0 * std::cos(3.141592653589793238462643383279 * (double)m / (double)h) - 2.0);
+  DT_TRY(dalloc(s, &tb.tw_row, N));
+  DT_TRY(dalloc(s, &tb.post, N));
+  DT_TRY(dalloc(s, &tb.tw_col, h));
+  DT_TRY(dalloc(s, &tb.omega, h));
+  DT_TRY(dalloc(s, &tb.lx, N + 1));
+  DT_TRY(dalloc(s, &tb.ly, h));
+  DT_CUDA(cudaMemcpy(tb.tw_row, a.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.post, b.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.tw_col, c.data(), h * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.omega, o.data(), h * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.lx, lx.data(), (N + 1) * sizeof(T), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.ly, ly.data(), h * sizeof(T), cudaMemcpyHostToDevice));
+  return DT_OK;
+}
+
+template <class T>
+static dt_status make_lane(dt_flex* s, Lane<T>& L) {
+  size_t n = s->n;
+  for (T** p : {&L.d, &L.c, &L.x, &L.r, &L.z, &L.p, &L.ap, &L.J, &L.wt[0], &L.wt[1], &L.wt[2], &L.left, &L.part})
+    DT_TRY(dalloc(s, p, n));
+  DT_TRY(dalloc(s, &L.half, (size_t)s->h * s->N));
+  DT_TRY(make_tables(s, L.tab));
+  DT_TRY(dalloc(s, &L.S, 1));
+  DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
+  return DT_OK;
+}
+
+template <class T>
+static void free_graphs(Lane<T>& L) {
+  for (int k = 0; k < 2; ++k) {
+    if (L.exec[k]) cudaGraphExecDestroy(L.exec[k]);
+    if (L.graph[k]) cudaGraphDestroy(L.graph[k]);
+    L.exec[k] = nullptr;
+    L.graph[k] = nullptr;
+  }
+}
+
+static unsigned int ew_grid(const dt_flex* s) { return std::max(1u, std::min<unsigned int>(ceil_div(s->n, 256), (unsigned)s->sms * 8)); }
+
+template <class T>
+static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* part, const T* d, const T* c, const T* rb, T* y,
+                         Scalars* S, cudaStream_t st) {
+  dim3 grid(ceil_div(s->w, TBX), ceil_div(s->h, TBY)), block(TBX, TTY);
+  T inv = (T)(1.0 / (s->dx * s->dx));
+  switch (mode) {
+    case AP_DOT: k_apply<T, AP_DOT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case RESID: k_apply<T, RESID><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case JAC_LEFT: k_apply<T, JAC_LEFT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case JAC_FINAL: k_apply<T, JAC_FINAL><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case PLAIN: k_apply<T, PLAIN><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case BEND: k_apply<T, BEND><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+  }
+}
+
+// Columns per block of the column pass: at least one warp, at most 1024 threads and 96 KB.
+static int cols_per_block(int h, size_t elem) {
+  int cpb = std::max(1, 256 / h);
+  while (cpb < 8 && cpb * 2 * h <= 8192 && (size_t)cpb * 2 * h * elem <= 98304) cpb *= 2;
+  return cpb;
+}
+
+// One spectral solve of one bank level: out (op)= S_k (in * wt) (* wt).
+template <class T>
+static void launch_spectral(dt_flex* s, Lane<T>& L, const T* in, const T* wt, T* out, int inv_mode, int level, Scalars* S,
+                            cudaStream_t st) {
+  using C = cplx<T>;
+  int N = s->N;
+  int RB = rows_per_block(N);
+  unsigned int rgrid = ceil_div(s->h, RB);
+  int rthreads = RB * N / 8;
+  size_t rsmem = (size_t)RB * N * sizeof(C);
+  if (wt)
+    k_rows_fwd<T, true><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row, L.tab.post, S);
+  else
+    k_rows_fwd<T, false><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row, L.tab.post, S);
+  int cpb = cols_per_block(s->h, sizeof(C));
+  unsigned int cgrid = ceil_div(N, cpb);
+  int cthreads = cpb * s->h / 8;
+  size_t csmem = (size_t)cpb * s->h * sizeof(C);
+  k_cols<T><<<cgrid, cthreads, csmem, st>>>(N, s->h, L.half, L.tab.tw_col, L.tab.omega, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S,
+                                            level);
+  switch (inv_mode) {
+    case INV_STORE:
+      k_rows_inv<T, INV_STORE><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      break;
+    case INV_STORE_W:
+      k_rows_inv<T, INV_STORE_W><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      break;
+    case INV_ACCUM:
+      k_rows_inv<T, INV_ACCUM><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      break;
+    case INV_STORE_DOT:
+      k_rows_inv<T, INV_STORE_DOT><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, in, L.tab.tw_row, L.tab.post, s->partials, S);
+      break;
+  }
+}
+
+// z = M^-1 r with r.z and max|z| reduced into S (finish_precond). levels 1: one spectral solve at
+// node_d[0]; levels 3: the reference's bank inside damped Jacobi sweeps (flexure.rs:1630-1651).
+template <class T>
+static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int levels, cudaStream_t st) {
+  if (levels == 1) {
+    launch_spectral<T>(s, L, r, nullptr, z, INV_STORE_DOT, 0, L.S, st);
+    return;
+  }
+  launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, r, L.left, L.S, st);  // left = r - A(J r)
+  for (int k = 0; k < 3; ++k)  // part = sum_k w_k S_k(w_k left)
+    launch_spectral<T>(s, L, L.left, L.wt[k], L.part, k == 0 ? INV_STORE_W : INV_ACCUM, k, L.S, st);
+  launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, r, z, L.S, st);  // z = u + J(r - A u)
+}
+
+// One PCG iteration (flexure.rs:1709-1738): the body of the device loop.
+template <class T>
+static void launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st) {
+  launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st);
+  k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S);
+  launch_precondition<T>(s, L, L.r, L.z, levels, st);
+  k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S);
+}
+
+// The loop graph: k_arm -> WHILE(iteration) -> k_disarm. Built once per lane and level count.
+template <class T>
+static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* out) {
+  int li = levels == 3 ? 1 : 0;
+  if (L.exec[li]) {
+    *out = L.exec[li];
+    return DT_OK;
+  }
+  cudaGraph_t g;
+  DT_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle handle;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+  unsigned long long hv = (unsigned long long)handle;
+  Scalars* Sp = L.S;
+  cudaKernelNodeParams kp = {};
+  void* arm_args[] = {&Sp, &hv};
+  kp.func = (void*)k_arm;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(1);
+  kp.kernelParams = arm_args;
+  cudaGraphNode_t n_arm, n_loop, n_disarm;
+  DT_CUDA(cudaGraphAddKernelNode(&n_arm, g, nullptr, 0, &kp));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  launch_iteration<T>(s, L, levels, s->stream);
+  cudaGraph_t captured;
+  DT_CUDA(cudaStreamEndCapture(s->stream, &captured));
+  void* dis_args[] = {&Sp};
+  kp.func = (void*)k_disarm;
+  kp.kernelParams = dis_args;
+  DT_CUDA(cudaGraphAddKernelNode(&n_disarm, g, &n_loop, 1, &kp));
+  cudaGraphExec_t exec;
+  DT_CUDA(cudaGraphInstantiate(&exec, g, 0));
+  L.graph[li] = g;
+  L.exec[li] = exec;
+  *out = exec;
+  return DT_OK;
+}
+
+// The preconditioner set-up of a lane for its d, c: the bank (or the mean level), and for three
+// levels the per-cell blend and Jacobi weights. Returns the level count (one host sync).
+template <class T>
+static dt_status setup_precond(dt_flex* s, Lane<T>& L, int precond, int* levels) {
+  cudaStream_t st = s->stream;
+  k_stats<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, L.c, s->dx, precond == DT_PRECOND_MEAN_D, s->partials, L.S);
+  int lv = 1;
+  DT_CUDA(cudaMemcpyAsync(&lv, &L.S->levels, sizeof(int), cudaMemcpyDeviceToHost, st));
+  DT_CUDA(cudaStreamSynchronize(st));
+  if (lv == 3) k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S);
+  DT_CUDA(cudaGetLastError());
+  *levels = lv;
+  return DT_OK;
+}
+
+struct HostProblem {
+  double tol;
+  int max_it;
+  int rule;
+  int n;
+};
+__global__ void k_put_problem(Scalars* S, HostProblem p) {
+  S->tol = p.tol;
+  S->max_it = p.max_it;
+  S->rule = p.rule;
+  S->n = p.n;
+}
+
+// PCG of lane L from its x (guess), r = b - A x and S->rr, S->bb already set: the first
+// preconditioning, p = z, then the device loop.
+template <class T>
+static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels) {
+  cudaStream_t st = s->stream;
+  k_begin<<<1, 1, 0, st>>>(L.S);
+  launch_precondition<T>(s, L, L.r, L.z, levels, st);
+  k_initial_result<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.z, L.S);
+  DT_CUDA(cudaMemcpyAsync(L.p, L.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  cudaGraphExec_t exec;
+  DT_TRY(loop_exec<T>(s, L, levels, &exec));
+  DT_CUDA(cudaGraphLaunch(exec, st));
+  return DT_OK;
+}
+
+static dt_status read_scalars(dt_flex* s, const Scalars* S, Scalars* out) {
+  DT_CUDA(cudaMemcpyAsync(out, S, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  return DT_OK;
+}
+
+// r = b - A x in FP64 with ||r||^2 into S->rr.
+static void resid64(dt_flex* s) {
+  Lane<double>& L = s->L64;
+  launch_apply<double>(s, RESID, L.x, nullptr, nullptr, L.d, L.c, s->b64, L.r, L.S, s->stream);
+}
+
+// ||b||^2 into S->bb
+template <class T>
+static void norm_b(dt_flex* s, const T* b, Scalars* S) {
+  k_dot<T><<<ew_grid(s), 256, 0, s->stream>>>(s->n, b, b, s->partials, S, SITE_DOT);
+  k_take_bb<<<1, 1, 0, s->stream>>>(S);
+}
+
+static dt_status warm_or_cold(dt_flex* s, bool warm) {
+  Lane<double>& L = s->L64;
+  cudaStream_t st = s->stream;
+  if (!warm) {
+    k_fill<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, 0.0);
+  }
+  resid64(s);  // r = b - A x (r = b for x = 0)
+  if (warm) {
+    k_warm_decide<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, L.S);
+    k_warm_record<<<1, 1, 0, st>>>(L.S, s->warm);
+  } else {
+    WarmInfo none = {0, 1.0};
+    DT_CUDA(cudaMemcpyAsync(s->warm, &none, sizeof none, cudaMemcpyHostToDevice, st));
+  }
+  return DT_OK;
+}
+
+static dt_status fill_report(dt_flex* s, const Scalars& h, int iterations, int refinements, dt_report* rep) {
+  WarmInfo wi;
+  DT_CUDA(cudaMemcpy(&wi, s->warm, sizeof wi, cudaMemcpyDeviceToHost));
+  if (!rep) return DT_OK;
+  rep->iterations = iterations;
+  rep->error_m = h.err;
+  rep->refinements = refinements;
+  rep->warm_start_accepted = wi.accepted;
+  rep->warm_start_rel_residual = wi.rel;
+  return DT_OK;
+}
+
+// The FP64 solve; inputs in L64.d, L64.c, b64, and the guess in L64.x when warm.
+static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_report* rep) {
+  Lane<double>& L = s->L64;
+  cudaStream_t st = s->stream;
+  int levels = 1;
+  DT_TRY(setup_precond<double>(s, L, p->precond, &levels));
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n});
+  norm_b<double>(s, s->b64, L.S);
+  DT_TRY(warm_or_cold(s, warm));
+  DT_TRY(run_pcg<double>(s, L, levels));
+  Scalars h;
+  DT_TRY(read_scalars(s, L.S, &h));
+  int iterations = h.it;
+  int stop = h.stop;
+  double err = h.err;
+  // the true residual of the answer
+  resid64(s);
+  DT_TRY(read_scalars(s, L.S, &h));
+  h.err = err;
+  DT_TRY(fill_report(s, h, iterations, 0, rep));
+  if (rep) {
+    rep->converged = stop == STOP_CONVERGED;
+    rep->rel_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
+  }
+  if (stop == STOP_NONFINITE) {
+    set_error("flexure solve: a non-finite value appeared");
+    return DT_NONFINITE;
+  }
+  return stop == STOP_CONVERGED ? DT_OK : DT_NOT_CONVERGED;
+}
+
+// FP32 inner PCG inside FP64 iterative refinement. The outer loop stops on the FP64 relative (or
+// RMS) residual; each inner solve works on the residual scaled to unit RMS and stops at a
+// relative residual of max(inner_tol, 0.3 tol / current) (capped at 0.5): the last refinement
+// needs only the reduction that is left.
+static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_report* rep) {
+  Lane<double>& L = s->L64;
+  Lane<float>& F = s->L32;
+  cudaStream_t st = s->stream;
+  if (p->stop == DT_STOP_MAX_Z) {
+    set_error("flexure solve: the mixed-precision path stops on a residual rule (DT_STOP_REL_RESIDUAL or DT_STOP_RMS_RESIDUAL)");
+    return DT_UNSUPPORTED;
+  }
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d);
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c);
+  int levels = 1;
+  DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n});
+  norm_b<double>(s, s->b64, L.S);
+  DT_TRY(warm_or_cold(s, warm));
+  int iterations = 0, refinements = 0;
+  Scalars h, hf;
+  hf.err = 0.0;
+  hf.stop = STOP_RUNNING;
+  bool converged = false, nonfinite = false;
+  for (;;) {
+    DT_TRY(read_scalars(s, L.S, &h));
+    if (!std::isfinite(h.rr) || !std::isfinite(h.bb)) {
+      nonfinite = true;
+      break;
+    }
+    double rel = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
+    double lim = p->stop == DT_STOP_REL_RESIDUAL ? p->tol : p->tol * std::sqrt((double)s->n / std::max(h.bb, 1e-300));
+    if (h.bb <= 0 || rel <= lim) {
+      converged = true;
+      break;
+    }
+    if (refinements >= p->max_refinements || iterations >= p->max_iterations) break;
+    double itol = std::min(0.5, std::max(p->inner_tol, 0.3 * lim / rel));
+    k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale);
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n});
+    norm_b<float>(s, F.r, F.S);
+    k_rr_is_bb<<<1, 1, 0, st>>>(F.S);  // x = 0: r = b
+    DT_TRY(run_pcg<float>(s, F, levels));
+    k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale);
+    resid64(s);
+    DT_TRY(read_scalars(s, F.S, &hf));
+    iterations += hf.it;
+    ++refinements;
+    if (hf.stop == STOP_NONFINITE) {
+      nonfinite = true;
+      break;
+    }
+  }
+  DT_TRY(read_scalars(s, L.S, &h));
+  h.err = hf.err;
+  DT_TRY(fill_report(s, h, iterations, refinements, rep));
+  if (rep) {
+    rep->converged = converged;
+    rep->rel_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
+  }
+  if (nonfinite) {
+    set_error("flexure solve: a non-finite value appeared");
+    return DT_NONFINITE;
+  }
+  return converged ? DT_OK : DT_NOT_CONVERGED;
+}
+
+}  // namespace dt
+
+using namespace dt;
+
+// =============================================================================================
+// C ABI
+
+extern "C" {
+
+const char* dt_last_error(void) { return dt::last_error(); }
+
+int dt_device_info(char* name, int len) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    if (name && len > 0) name[0] = 0;
+    return 0;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, 0) != cudaSuccess) return 0;
+  if (name && len > 0) snprintf(name, len, "%s (sm_%d%d, %d SMs)", p.name, p.major, p.minor, p.multiProcessorCount);
+  return 1;
+}
+
+void dt_flex_default_params(dt_flex_params* p) {
+  if (!p) return;
+  p->precond = DT_PRECOND_REFERENCE;
+  p->stop = DT_STOP_MAX_Z;
+  p->precision = DT_PREC_FP64;
+  p->warm_start = DT_WARM_NONE;
+  p->tol = 2.0;            // FlexureParams::default tolerance_m (flexure.rs:224)
+  p->max_iterations = 60;  // FlexureParams::default max_iterations (flexure.rs:225)
+  p->inner_tol = 1e-5;
+  p->max_refinements = 8;
+}
+
+dt_status dt_flex_destroy(dt_flex* s) {
+  if (!s) return DT_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_graphs(s->L64);
+  free_graphs(s->L32);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return DT_OK;
+}
+
+dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const double* metric_b, dt_flex** out) {
+  if (!out) {
+    set_error("dt_flex_create: out is NULL");
+    return DT_BAD_ARG;
+  }
+  *out = nullptr;
+  if (w < 2 || h < 2 || !(dx > 0.0) || !std::isfinite(dx)) {
+    set_error("dt_flex_create: bad raster %d x %d, dx %g", w, h, dx);
+    return DT_BAD_ARG;
+  }
+  if ((w & 1) || !is_pow2(w / 2) || !is_pow2(h) || w / 2 > 8192 || h > 8192) {
+    set_error("dt_flex_create: the device transforms need w/2 and h powers of two, at most 8192 (got %d x %d)", w, h);
+    return DT_UNSUPPORTED;
+  }
+  if (metric_a || metric_b) {
+    set_error("dt_flex_create: the sphere's row metric (RowMetric) has no device path in this build");
+    return DT_UNSUPPORTED;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    set_error("dt_flex_create: no CUDA device");
+    return DT_DEVICE_ERROR;
+  }
+  auto* s = new dt_flex();
+  s->w = w;
+  s->h = h;
+  s->N = w / 2;
+  s->dx = dx;
+  s->n = (size_t)w * h;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, 0) == cudaSuccess) s->sms = prop.multiProcessorCount;
+  dt_status st = DT_OK;
+  auto fail = [&](dt_status e) {
+    dt_flex_destroy(s);
+    return e;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("dt_flex_create: cudaStreamCreate failed");
+    return fail(DT_DEVICE_ERROR);
+  }
+  s->own_stream = true;
+  if ((st = make_lane<double>(s, s->L64)) != DT_OK) return fail(st);
+  if ((st = make_lane<float>(s, s->L32)) != DT_OK) return fail(st);
+  if ((st = dalloc(s, &s->b64, s->n)) != DT_OK) return fail(st);
+  size_t tiles = (size_t)ceil_div(w, TBX) * ceil_div(h, TBY);
+  size_t cap = std::max<size_t>(std::max<size_t>(tiles, (size_t)s->sms * 8), (size_t)h) * 4;
+  if ((st = dalloc(s, &s->partials, cap)) != DT_OK) return fail(st);
+  if ((st = dalloc(s, &s->scale, 1)) != DT_OK) return fail(st);
+  if ((st = dalloc(s, &s->warm, 1)) != DT_OK) return fail(st);
+  int big = 200 * 1024;
+  cudaFuncSetAttribute(k_rows_fwd<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_rows_fwd<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_rows_fwd<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_rows_fwd<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_cols<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+  cudaFuncSetAttribute(k_cols<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+#define DT_SETINV(T, M) cudaFuncSetAttribute(k_rows_inv<T, M>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)
+  DT_SETINV(double, INV_STORE);
+  DT_SETINV(double, INV_STORE_W);
+  DT_SETINV(double, INV_ACCUM);
+  DT_SETINV(double, INV_STORE_DOT);
+  DT_SETINV(float, INV_STORE);
+  DT_SETINV(float, INV_STORE_W);
+  DT_SETINV(float, INV_ACCUM);
+  DT_SETINV(float, INV_STORE_DOT);
+#undef DT_SETINV
+  if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+    set_error("dt_flex_create: cudaEventCreate failed");
+    return fail(DT_DEVICE_ERROR);
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_error("dt_flex_create: %s", cudaGetErrorString(e));
+    return fail(DT_DEVICE_ERROR);
+  }
+  *out = s;
+  return DT_OK;
+}
+
+dt_status dt_flex_set_stream(dt_flex* s, void* stream) {
+  if (!s) return DT_BAD_ARG;
+  cudaStreamSynchronize(s->stream);
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return DT_DEVICE_ERROR;
+    s->own_stream = true;
+  }
+  return DT_OK;
+}
+
+static dt_status check_params(const dt_flex_params* p) {
+  if (!p) {
+    set_error("flexure solve: params is NULL");
+    return DT_BAD_ARG;
+  }
+  if (p->precond != DT_PRECOND_REFERENCE && p->precond != DT_PRECOND_MEAN_D) {
+    set_error("flexure solve: unknown preconditioner %d", p->precond);
+    return DT_BAD_ARG;
+  }
+  if (p->stop < DT_STOP_MAX_Z || p->stop > DT_STOP_RMS_RESIDUAL || !(p->tol >= 0.0) || p->max_iterations < 0) {
+    set_error("flexure solve: bad stopping rule (rule %d, tol %g, max_iterations %d)", p->stop, p->tol, p->max_iterations);
+    return DT_BAD_ARG;
+  }
+  if (p->precision != DT_PREC_FP64 && p->precision != DT_PREC_MIXED) {
+    set_error("flexure solve: unknown precision %d", p->precision);
+    return DT_BAD_ARG;
+  }
+  if (p->warm_start != DT_WARM_NONE && p->warm_start != DT_WARM_GIVEN) {
+    set_error("flexure solve: warm start %d needs dt_unet (use dt_unet_flex_solve)", p->warm_start);
+    return DT_UNSUPPORTED;
+  }
+  return DT_OK;
+}
+
+// The solve on inputs already in L64.d, L64.c, b64 (and the guess in L64.x).
+static dt_status solve_loaded(dt_flex* s, const dt_flex_params* p, dt_report* rep) {
+  bool warm = p->warm_start != DT_WARM_NONE;
+  cudaEventRecord(s->ev0, s->stream);
+  dt_status st = p->precision == DT_PREC_MIXED ? solve_mixed(s, p, warm, rep) : solve_fp64(s, p, warm, rep);
+  cudaEventRecord(s->ev1, s->stream);
+  cudaError_t e = cudaEventSynchronize(s->ev1);
+  if (e != cudaSuccess) {
+    set_error("flexure solve: %s", cudaGetErrorString(e));
+    return DT_DEVICE_ERROR;
+  }
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  if (rep) rep->device_ms = ms;
+  return st;
+}
+
+dt_status dt_flex_solve_dev(dt_flex* s, const double* d, const double* c, const double* b, double* x_inout,
+                            const dt_flex_params* p, dt_report* rep) {
+  if (!s || !d || !c || !b || !x_inout) {
+    set_error("dt_flex_solve_dev: NULL argument");
+    return DT_BAD_ARG;
+  }
+  DT_TRY(check_params(p));
+  size_t bytes = s->n * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->L64.d, d, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->L64.c, c, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->b64, b, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  if (p->warm_start == DT_WARM_GIVEN) DT_CUDA(cudaMemcpyAsync(s->L64.x, x_inout, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  dt_status st = solve_loaded(s, p, rep);
+  if (st == DT_OK || st == DT_NOT_CONVERGED) {
+    DT_CUDA(cudaMemcpyAsync(x_inout, s->L64.x, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    DT_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
+}
+
+dt_status dt_flex_solve(dt_flex* s, const double* d, const double* c, const double* b, double* x_inout, const dt_flex_params* p,
+                        dt_report* rep) {
+  if (!s || !d || !c || !b || !x_inout) {
+    set_error("dt_flex_solve: NULL argument");
+    return DT_BAD_ARG;
+  }
+  DT_TRY(check_params(p));
+  size_t bytes = s->n * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->L64.d, d, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->L64.c, c, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->b64, b, bytes, cudaMemcpyHostToDevice, s->stream));
+  if (p->warm_start == DT_WARM_GIVEN) DT_CUDA(cudaMemcpyAsync(s->L64.x, x_inout, bytes, cudaMemcpyHostToDevice, s->stream));
+  dt_status st = solve_loaded(s, p, rep);
+  if (st == DT_OK || st == DT_NOT_CONVERGED) {
+    DT_CUDA(cudaMemcpyAsync(x_inout, s->L64.x, bytes, cudaMemcpyDeviceToHost, s->stream));
+    DT_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
+}
+
+static dt_status apply_host(dt_flex* s, int mode, const double* d, const double* c, const double* v, double* y) {
+  if (!s || !d || !v || !y || (mode == PLAIN && !c)) {
+    set_error("flexure operator: NULL argument");
+    return DT_BAD_ARG;
+  }
+  size_t bytes = s->n * sizeof(double);
+  Lane<double>& L = s->L64;
+  DT_CUDA(cudaMemcpyAsync(L.d, d, bytes, cudaMemcpyHostToDevice, s->stream));
+  if (c) DT_CUDA(cudaMemcpyAsync(L.c, c, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(L.p, v, bytes, cudaMemcpyHostToDevice, s->stream));
+  launch_apply<double>(s, mode, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, s->stream);
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(y, L.ap, bytes, cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  return DT_OK;
+}
+
+dt_status dt_flex_operator(dt_flex* s, const double* d, const double* c, const double* v, double* y) {
+  return apply_host(s, PLAIN, d, c, v, y);
+}
+
+dt_status dt_flex_bend(dt_flex* s, const double* d, const double* v, double* y) { return apply_host(s, BEND, d, nullptr, v, y); }
+
+dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, const double* r, double* z, int precond, int precision) {
+  if (!s || !d || !c || !r || !z) {
+    set_error("dt_flex_precondition: NULL argument");
+    return DT_BAD_ARG;
+  }
+  size_t bytes = s->n * sizeof(double);
+  cudaStream_t st = s->stream;
+  Lane<double>& L = s->L64;
+  DT_CUDA(cudaMemcpyAsync(L.d, d, bytes, cudaMemcpyHostToDevice, st));
+  DT_CUDA(cudaMemcpyAsync(L.c, c, bytes, cudaMemcpyHostToDevice, st));
+  DT_CUDA(cudaMemcpyAsync(L.r, r, bytes, cudaMemcpyHostToDevice, st));
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n});
+  if (precision == DT_PREC_MIXED) {
+    Lane<float>& F = s->L32;
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d);
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c);
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r);
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n});
+    int levels;
+    DT_TRY(setup_precond<float>(s, F, precond, &levels));
+    k_reset<<<1, 1, 0, st>>>(F.S);
+    launch_precondition<float>(s, F, F.r, F.z, levels, st);
+    k_convert<float, double><<<ew_grid(s), 256, 0, st>>>(s->n, F.z, L.z);
+  } else {
+    int levels;
+    DT_TRY(setup_precond<double>(s, L, precond, &levels));
+    k_reset<<<1, 1, 0, st>>>(L.S);
+    launch_precondition<double>(s, L, L.r, L.z, levels, st);
+  }
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(z, L.z, bytes, cudaMemcpyDeviceToHost, st));
+  DT_CUDA(cudaStreamSynchronize(st));
+  return DT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,114 @@
+/* deeptime_gpu.h - the C ABI of the B200 backend for deep-time's per-timestep elliptic solves.
+ *
+ * Two solves, each behind an opaque handle that owns its device buffers, FFT tables, multigrid
+ * levels and CUDA graphs for one raster shape (w x h cells of dx metres; x wraps, the first and
+ * last rows are closed):
+ *
+ *   flexure    (L D L + C) x = b, L the 5-point Laplacian; PCG with a spectral preconditioner.
+ *              Replaces flexure::Solver (crates/deeptime-core/src/surface/flexure.rs:1471-1741):
+ *              dt_flex_create      <- Solver::with_metric   (flexure.rs:1528)
+ *              dt_flex_solve       <- Solver::solve         (flexure.rs:1680-1687)
+ *              dt_flex_operator    <- Solver::operator      (flexure.rs:1606)
+ *              dt_flex_bend        <- Solver::bend          (flexure.rs:1598)
+ *   diffusion  (I + dt L_kd) h' = h, L_kd the variable-coefficient 5-point flux Laplacian; CG
+ *              preconditioned by one multigrid V-cycle.
+ *              dt_diff_solve       <- diffusion::solve      (crates/deeptime-core/src/surface/diffusion.rs:77-85)
+ *                                     with DiffusionSolver::Multigrid (multigrid::cg_on,
+ *                                     surface/diffusion/multigrid.rs:562-763)
+ *
+ * Conventions. Host arrays are row-major (x fastest), w*h doubles, borrowed for the call. The
+ * `_dev` variants take device pointers and run on the handle's stream. Every call returns a status;
+ * no exception crosses the boundary; dt_last_error() gives the calling thread's last message.
+ * A handle is not thread-safe: use one per thread (or per stream).
+ * There is no CPU fallback: without a usable CUDA device every entry point returns
+ * DT_DEVICE_ERROR.
+ */
+#ifndef DEEPTIME_GPU_H
+#define DEEPTIME_GPU_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  DT_OK = 0,
+  DT_NOT_CONVERGED = 1, /* the iteration cap was reached (the reference's converged = false) */
+  DT_NONFINITE = 2,     /* a non-finite value appeared (flexure.rs:2571-2575 maps this to InvalidState) */
+  DT_OOM = 3,
+  DT_BAD_ARG = 4,
+  DT_DEVICE_ERROR = 5,
+  DT_UNSUPPORTED = 6    /* a shape or option this build does not handle; see dt_last_error() */
+} dt_status;
+
+enum { DT_PRECOND_REFERENCE = 0, /* 3-level ln(alpha) bank inside damped Jacobi sweeps, flexure.rs:1352-1468 */
+       DT_PRECOND_MEAN_D = 1 };  /* one spectral solve at the mean rigidity and mean restoring density */
+enum { DT_STOP_MAX_Z = 0,        /* the reference's: max |z| < tol metres (flexure.rs:1727-1732) */
+       DT_STOP_REL_RESIDUAL = 1, /* ||b - A x||_2 / ||b||_2 <= tol */
+       DT_STOP_RMS_RESIDUAL = 2 };/* the reference diffusion's: ||r||_2^2 <= tol^2 n (multigrid.rs:620) */
+enum { DT_PREC_FP64 = 0,         /* PCG entirely in FP64 */
+       DT_PREC_MIXED = 1 };      /* FP32 inner PCG inside FP64 iterative refinement */
+enum { DT_WARM_NONE = 0,         /* start from x = 0 (the reference) */
+       DT_WARM_GIVEN = 1,        /* start from x_inout's contents */
+       DT_WARM_UNET = 2 };       /* start from the loaded U-Net's prediction, when it beats x = 0 */
+enum { DT_CYCLE_JACOBI = 0,      /* the reference's V-cycle: damped Jacobi, omega 0.8, nu 2, to <= 64 cells */
+       DT_CYCLE_RBGS = 1 };      /* red-black Gauss-Seidel V(2,2) to a 16 x 8 coarsest level */
+enum { DT_DIFF_FP64_CG_FP32_CYCLE = 0, /* the reference's split: FP64 CG, FP32 cycle */
+       DT_DIFF_FP64 = 1,               /* FP64 CG and FP64 cycle */
+       DT_DIFF_MIXED = 2 };            /* FP32 inner CG + FP32 cycle inside FP64 refinement */
+
+typedef struct {
+  int precond;          /* DT_PRECOND_* */
+  int stop;             /* DT_STOP_MAX_Z or DT_STOP_REL_RESIDUAL */
+  int precision;        /* DT_PREC_* */
+  int warm_start;       /* DT_WARM_* */
+  double tol;           /* metres (MAX_Z) or relative residual */
+  int max_iterations;   /* PCG iterations (summed over refinements in MIXED) */
+  double inner_tol;     /* MIXED: inner relative residual, at least this (default 1e-5) */
+  int max_refinements;  /* MIXED: outer FP64 refinements (default 8) */
+} dt_flex_params;
+
+typedef struct {
+  /* the reference's SolveReport (flexure.rs:947-952) */
+  int iterations;       /* PCG iterations (all refinements) */
+  double error_m;       /* the last max |z| (the reference's error estimate), metres */
+  int converged;
+  /* additions */
+  double rel_residual;  /* ||b - A x|| / ||b|| at exit (recomputed in FP64) */
+  int refinements;      /* MIXED: FP64 refinement steps taken */
+  int warm_start_accepted;
+  double warm_start_rel_residual; /* ||b - A x0|| / ||b|| of the offered first guess */
+  double device_ms;     /* device time of the solve (CUDA events on the handle's stream) */
+} dt_report;
+
+typedef struct dt_flex dt_flex;
+typedef struct dt_diff dt_diff;
+
+void dt_flex_default_params(dt_flex_params* p);
+
+/* metric_a (h values) and metric_b (h + 1 values) select the sphere's row metric (RowMetric,
+ * flexure.rs:964-1010); pass NULL for the block metric. */
+dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const double* metric_b, dt_flex** out);
+dt_status dt_flex_destroy(dt_flex* s);
+/* Binds the handle to a CUDA stream (cudaStream_t passed as void*); NULL = the handle's own. */
+dt_status dt_flex_set_stream(dt_flex* s, void* stream);
+/* d = D/g (kg m), c = restoring density (kg/m^3), b = load (kg/m^2); x in metres. With
+ * DT_WARM_GIVEN, x_inout holds the first guess on entry. */
+dt_status dt_flex_solve(dt_flex* s, const double* d, const double* c, const double* b, double* x_inout,
+                        const dt_flex_params* p, dt_report* rep);
+dt_status dt_flex_solve_dev(dt_flex* s, const double* d, const double* c, const double* b, double* x_inout,
+                            const dt_flex_params* p, dt_report* rep);
+/* y = (L D L + C) v and y = L (D L v) (host arrays). */
+dt_status dt_flex_operator(dt_flex* s, const double* d, const double* c, const double* v, double* y);
+dt_status dt_flex_bend(dt_flex* s, const double* d, const double* v, double* y);
+/* z = M^-1 r with the chosen preconditioner (host arrays); for tests of the transforms. */
+dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, const double* r, double* z, int precond,
+                               int precision);
+
+const char* dt_last_error(void);
+/* Library and device facts: 1 when a CUDA device is usable, with its name. */
+int dt_device_info(char* name, int len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
