@@ -1,0 +1,361 @@
+"""Benchmark: flexure solves per second to a relative residual of 1e-8 on a 4096 x 2048 raster.
+
+Workload (the mixed-precision configuration): dx = 2.5 km, rigidity D = 10^(21 + 3u) with u
+seeded white noise Gaussian-smoothed over 32 cells and rescaled to [0, 1], load q = 2700 g h with
+h a seeded |k|^-2 Gaussian random field of std 1500 m, restoring density 3300 kg/m^3; PCG from
+x = 0 (or the U-Net's first guess) to ||b - A x|| / ||b|| <= 1e-8. A step is one solve of one
+input set; input sets are generated up front and cycled, each vector 67 MB, so the working set
+(several hundred MB) is larger than the 126 MB L2 and no flush is needed between steps.
+
+One process per GPU (torchrun for N > 1). The solves are independent, so N GPUs run N replicas
+(weak scaling, no collective on the data path); rank 0 prints one JSON line with the whole-job
+throughput over the max-over-ranks device time.
+
+  value     solves/s with inputs resident in HBM (dt_flex_solve_dev, CUDA events, barrier and
+            synchronize on both sides)
+  e2e       the same through dt_flex_solve from pinned host buffers: the H2D copy of d, c, b and
+            the D2H copy of x are inside the timed region
+  roofline  the dominant kernel's algorithmic bytes per launch / its event-timed launch duration
+  cpu_baseline  the oracle (a C++ restatement of the reference's CPU solver, FP64, its own
+            3-level bank preconditioner) on the host's cores, a bounded sample extrapolated
+--impl reference times that CPU restatement alone, as the reference arm.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "deep-time_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+W, H, DX, SIGMA = 4096, 2048, 2500.0, 32.0
+TOL = 1e-8
+KERNEL_NAMES = ["flex_apply", "cg_update", "cg_direction", "fft_rows_fwd", "dct_cols_divide_idct", "fft_rows_inv_dot",
+                "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_accumulate"]
+METRIC = "flexure solves/s to relative residual 1e-8 @4096x2048 (time-to-1e-8 per solve = 1000/value ms)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
+    ap.add_argument("--precond", default="reference", choices=["reference", "mean_d"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v, world):
+    if world <= 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_inputs(k, seed0=1000):
+    from deeptime_gpu import inputs as I
+
+    return [I.flexure_problem(W, H, SIGMA, seed0 + 100 * i) for i in range(k)]
+
+
+def oracle_cpu_baseline(d, c, b, its_needed, max_seconds=30.0):
+    """The oracle's FP64 solve (the reference's preconditioner) at full size: setup and per-iteration
+    time from runs capped at 1 and 3 iterations, extrapolated to the iterations the same algorithm
+    needs to reach 1e-8 (its_needed)."""
+    from oracle import oracle as O
+
+    def timed(its):
+        t = time.perf_counter()
+        O.flex_solve(d, c, b, DX, TOL, its, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+        return time.perf_counter() - t
+
+    t1 = timed(1)
+    t3 = timed(3)
+    per_it = max((t3 - t1) / 2.0, 1e-9)
+    setup = max(t1 - per_it, 0.0)
+    seconds = setup + per_it * its_needed
+    return {"value": 1.0 / seconds, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": (f"oracle FP64 PCG with the reference's 3-level bank + Jacobi preconditioner on {W}x{H}: "
+                       f"setup {setup:.2f} s and {per_it:.2f} s/iteration measured from solves capped at 1 and 3 "
+                       f"iterations, extrapolated to {its_needed} iterations (the count the same algorithm takes to "
+                       f"1e-8 on the GPU); OpenMP on all {os.cpu_count()} host threads"),
+            "seconds_per_solve": seconds}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as O
+
+    O.build() if not os.path.exists(O.LIB_PATH) else None
+    d, c, b = make_inputs(1)[0]
+    # iterations the reference algorithm needs (one full solve, in the warm-up)
+    t = time.perf_counter()
+    x, rep = O.flex_solve(d, c, b, DX, TOL, 2000, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+    full = time.perf_counter() - t
+    its = rep["iterations"]
+    times = []
+    for k in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.flex_solve(d, c, b, DX, TOL, 3, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+        el = time.perf_counter() - t0
+        if k >= args.warmup:
+            times.append(el)
+    t1 = time.perf_counter()
+    O.flex_solve(d, c, b, DX, TOL, 1, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+    one = time.perf_counter() - t1
+    per_it = max((statistics.median(times) - one) / 2.0, 1e-9)
+    seconds = max(one - per_it, 0.0) + per_it * its
+    value = 1.0 / seconds
+    sample = (f"each step: the oracle (C++/OpenMP restatement of the reference's flexure::Solver) solving {W}x{H} capped "
+              f"at 3 iterations; per-iteration time from those steps and a 1-iteration solve, extrapolated to the "
+              f"{its} iterations its full warm-up solve took to 1e-8 ({full:.1f} s measured)")
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * seconds, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 fields)", "impl": "reference",
+            "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
+                       "precision": "fp64", "preconditioner": "reference 3-level bank + Jacobi", "iterations": its,
+                       "full_solve_seconds": full},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_init(args.gpus)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import flexure as F
+
+    torch.cuda.set_device(local)
+    lib = L.lib()
+    stream = torch.cuda.Stream()
+    inputs = make_inputs(max(1, args.inputs), seed0=1000 + 7919 * rank)
+    dev = [tuple(torch.from_numpy(a).cuda() for a in inp) for inp in inputs]
+    x_dev = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+    sv = F.Solver(W, H, DX)
+    L.check(lib.dt_flex_set_stream(sv._h, ctypes.c_void_p(stream.cuda_stream)))
+    precond = L.PRECOND_REFERENCE if args.precond == "reference" else L.PRECOND_MEAN_D
+    mixed = F.params(precond=precond, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_MIXED, tol=TOL, max_iterations=20000)
+    plain = F.params(precond=L.PRECOND_MEAN_D, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_FP64, tol=TOL,
+                     max_iterations=20000)
+
+    def solve_dev(i, p):
+        d, c, b = dev[i % len(dev)]
+        rep = L.Report()
+        st = lib.dt_flex_solve_dev(sv._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(c.data_ptr()),
+                                   ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_dev.data_ptr()), ctypes.byref(p),
+                                   ctypes.byref(rep))
+        L.check(st)
+        return rep
+
+    def timed(fn, steps):
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        reps = [fn(i) for i in range(steps)]
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        return e0.elapsed_time(e1), reps
+
+    for i in range(args.warmup):
+        solve_dev(i, mixed)
+    with Clocks(local) as clk:
+        ms, reps = timed(lambda i: solve_dev(i, mixed), args.steps)
+    ms = max_over_ranks(ms, world)
+    its = [r.iterations for r in reps]
+    launches = sum(r.kernel_launches for r in reps)
+
+    # plain FP64 GPU PCG (mean-D preconditioner) on the same inputs: the comparison the target names
+    for i in range(1):
+        solve_dev(i, plain)
+    plain_steps = min(args.steps, 3)
+    pms, preps = timed(lambda i: solve_dev(i, plain), plain_steps)
+    pms = max_over_ranks(pms, world)
+
+    # end to end through dt_flex_solve from pinned host buffers
+    host = []
+    for d, c, b in inputs:
+        hs = [torch.from_numpy(a).pin_memory() for a in (d, c, b)]
+        host.append(hs)
+    x_host = torch.zeros((H, W), dtype=torch.float64).pin_memory()
+
+    def solve_host(i):
+        d, c, b = host[i % len(host)]
+        rep = L.Report()
+        st = lib.dt_flex_solve(sv._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(c.data_ptr()),
+                               ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_host.data_ptr()), ctypes.byref(mixed),
+                               ctypes.byref(rep))
+        L.check(st)
+        return rep
+
+    solve_host(0)
+    e2e_steps = min(args.steps, 4)
+    ems, _ = timed(solve_host, e2e_steps)
+    ems = max_over_ranks(ems, world)
+
+    # per-kernel launch durations (events) for the roofline
+    kms = (ctypes.c_double * 10)()
+    kbytes = (ctypes.c_double * 10)()
+    solve_dev(0, mixed)
+    L.check(lib.dt_flex_profile_kernels(sv._h, L.PREC_MIXED, 20, kms, kbytes))
+    levels3 = args.precond == "reference"
+    per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: 3, 4: 3, 9: 3} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 4: 1, 5: 1})
+    share = {k: kms[k] * cnt for k, cnt in per_it.items()}
+    top = max(share, key=share.get)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else None
+    peak = peaks["hbm_gbs"] if peaks else 6650.0
+    achieved = kbytes[top] / (kms[top] * 1e-3) / 1e9
+    traffic = read_traffic(KERNEL_NAMES[top])
+    kernels = {KERNEL_NAMES[k]: {"ms": kms[k], "GB/s": kbytes[k] / (kms[k] * 1e-3) / 1e9, "launches_per_iteration": cnt}
+               for k, cnt in per_it.items()}
+
+    value = world * args.steps / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic (seeded SplitMix64 fields)",
+        "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
+                   "method": f"mixed precision (FP32 inner PCG in FP64 refinement), "
+                             f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, zero first guess",
+                   "inputs": f"{len(inputs)} seeded input sets cycled, 201 MB each: larger than L2, no flush",
+                   "iterations_per_solve": statistics.mean(its), "replicas": world},
+        "plain_fp64_gpu": {"ms_per_solve": pms / plain_steps, "iterations": statistics.mean(r.iterations for r in preps),
+                           "method": "FP64 PCG, constant-mean-D spectral preconditioner",
+                           "speedup_of_value": (pms / plain_steps) / (ms / args.steps)},
+        "e2e": {"value": world * e2e_steps / (ems / 1e3), "unit": "solves/s",
+                "h2d_bytes_per_step": 3 * W * H * 8, "d2h_bytes_per_step": W * H * 8},
+        "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peaks else "fallback",
+                     "traffic": traffic, "algorithmic_bytes_per_launch": kbytes[top], "kernels": kernels},
+        "clocks": clk.summary(),
+        "gpu_launches": launches,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        from deeptime_gpu import flexure as F2  # noqa: F401
+
+        d, c, b = inputs[0]
+        ref_its = solve_dev(0, F.params(precond=L.PRECOND_REFERENCE, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_FP64,
+                                        tol=TOL, max_iterations=20000)).iterations
+        line["cpu_baseline"] = oracle_cpu_baseline(d, c, b, ref_its)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sv.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def read_traffic(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if one was captured."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+if __name__ == "__main__":
+    main()

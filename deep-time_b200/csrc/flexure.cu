@@ -134,9 +134,9 @@ __device__ void finish_precond(Scalars* S, double rz, double err) {
 
 // Bank::new from ln(alpha) extremes and the sums (flexure.rs:1361-1401); `mean_d` selects the
 // single mean level instead.
-__device__ void finish_stats(Scalars* S, double lo, double hi, double sum_c, double sum_d, double dx, bool mean_d) {
+__device__ void finish_stats(Scalars* S, double lo, double hi, double sum_c, double sum_d, double dx, bool mean_d, size_t cells) {
   const double RHO_MANTLE = 3300.0;
-  double n = (double)max(S->n, 1);
+  double n = (double)(cells > 0 ? cells : 1);
   S->lo = lo;
   S->hi = hi;
   S->sum_c = sum_c;
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(256) k_stats(size_t n, const T* __restrict__ d
   }
   const int kind[4] = {1, 1, 0, 0};
   if (reduce_partials<4>(acc, kind, partials, &S->ticket[SITE_STATS], gridDim.x) && threadIdx.x == 0)
-    finish_stats(S, -acc.v[0], acc.v[1], acc.v[2], acc.v[3], dx, mean_d != 0);
+    finish_stats(S, -acc.v[0], acc.v[1], acc.v[2], acc.v[3], dx, mean_d != 0, n);
 }
 
 // Per cell: the bank's weights (squares sum to one) and the damped Jacobi weight 1/2 / diag.
@@ -758,6 +758,17 @@ void set_error(const char* fmt, ...) {
 }
 const char* last_error() { return g_err; }
 
+// Kernel launches of the calling thread: eager ones, and those recorded into a graph body while
+// capturing (a body's kernels run once per loop pass).
+static thread_local long long g_launches = 0, g_captured = 0;
+static thread_local bool g_capturing = false;
+static inline void counted() {
+  if (g_capturing)
+    ++g_captured;
+  else
+    ++g_launches;
+}
+
 template <class T>
 struct Tables {
   cplx<T>* tw_row = nullptr;  // N = w/2 entries e^(-2 pi i t / N)
@@ -777,6 +788,7 @@ struct Lane {
   Scalars* S = nullptr;
   cudaGraph_t graph[2] = {nullptr, nullptr};  // [levels == 3]
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  long long body_kernels[2] = {0, 0};         // kernels in one pass of each loop body
 };
 
 static const long double PI_L = 3.14159265358979323846264338327950288L;
@@ -880,12 +892,12 @@ static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* 
   dim3 grid(ceil_div(s->w, TBX), ceil_div(s->h, TBY)), block(TBX, TTY);
   T inv = (T)(1.0 / (s->dx * s->dx));
   switch (mode) {
-    case AP_DOT: k_apply<T, AP_DOT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
-    case RESID: k_apply<T, RESID><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
-    case JAC_LEFT: k_apply<T, JAC_LEFT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
-    case JAC_FINAL: k_apply<T, JAC_FINAL><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
-    case PLAIN: k_apply<T, PLAIN><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
-    case BEND: k_apply<T, BEND><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); break;
+    case AP_DOT: k_apply<T, AP_DOT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case RESID: k_apply<T, RESID><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case JAC_LEFT: k_apply<T, JAC_LEFT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case JAC_FINAL: k_apply<T, JAC_FINAL><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case PLAIN: k_apply<T, PLAIN><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case BEND: k_apply<T, BEND><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
   }
 }
 
@@ -910,24 +922,25 @@ static void launch_spectral(dt_flex* s, Lane<T>& L, const T* in, const T* wt, T*
     k_rows_fwd<T, true><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row, L.tab.post, S);
   else
     k_rows_fwd<T, false><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row, L.tab.post, S);
+  counted();
   int cpb = cols_per_block(s->h, sizeof(C));
   unsigned int cgrid = ceil_div(N, cpb);
   int cthreads = cpb * s->h / 8;
   size_t csmem = (size_t)cpb * s->h * sizeof(C);
   k_cols<T><<<cgrid, cthreads, csmem, st>>>(N, s->h, L.half, L.tab.tw_col, L.tab.omega, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S,
-                                            level);
+                                            level); counted();
   switch (inv_mode) {
     case INV_STORE:
-      k_rows_inv<T, INV_STORE><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      k_rows_inv<T, INV_STORE><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S); counted();
       break;
     case INV_STORE_W:
-      k_rows_inv<T, INV_STORE_W><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      k_rows_inv<T, INV_STORE_W><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S); counted();
       break;
     case INV_ACCUM:
-      k_rows_inv<T, INV_ACCUM><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S);
+      k_rows_inv<T, INV_ACCUM><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, nullptr, L.tab.tw_row, L.tab.post, s->partials, S); counted();
       break;
     case INV_STORE_DOT:
-      k_rows_inv<T, INV_STORE_DOT><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, in, L.tab.tw_row, L.tab.post, s->partials, S);
+      k_rows_inv<T, INV_STORE_DOT><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, out, wt, in, L.tab.tw_row, L.tab.post, s->partials, S); counted();
       break;
   }
 }
@@ -950,9 +963,9 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
 template <class T>
 static void launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st) {
   launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st);
-  k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S);
+  k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); counted();
   launch_precondition<T>(s, L, L.r, L.z, levels, st);
-  k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S);
+  k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); counted();
 }
 
 // The loop graph: k_arm -> WHILE(iteration) -> k_disarm. Built once per lane and level count.
@@ -985,7 +998,11 @@ static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* 
   DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  g_capturing = true;
+  g_captured = 0;
   launch_iteration<T>(s, L, levels, s->stream);
+  g_capturing = false;
+  L.body_kernels[li] = g_captured;
   cudaGraph_t captured;
   DT_CUDA(cudaStreamEndCapture(s->stream, &captured));
   void* dis_args[] = {&Sp};
@@ -1005,11 +1022,14 @@ static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* 
 template <class T>
 static dt_status setup_precond(dt_flex* s, Lane<T>& L, int precond, int* levels) {
   cudaStream_t st = s->stream;
-  k_stats<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, L.c, s->dx, precond == DT_PRECOND_MEAN_D, s->partials, L.S);
+  k_stats<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, L.c, s->dx, precond == DT_PRECOND_MEAN_D, s->partials, L.S); counted();
   int lv = 1;
   DT_CUDA(cudaMemcpyAsync(&lv, &L.S->levels, sizeof(int), cudaMemcpyDeviceToHost, st));
   DT_CUDA(cudaStreamSynchronize(st));
-  if (lv == 3) k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S);
+  if (lv == 3) {
+    k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S);
+    counted();
+  }
   DT_CUDA(cudaGetLastError());
   *levels = lv;
   return DT_OK;
@@ -1030,23 +1050,45 @@ __global__ void k_put_problem(Scalars* S, HostProblem p) {
 
 // PCG of lane L from its x (guess), r = b - A x and S->rr, S->bb already set: the first
 // preconditioning, p = z, then the device loop.
-template <class T>
-static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels) {
-  cudaStream_t st = s->stream;
-  k_begin<<<1, 1, 0, st>>>(L.S);
-  launch_precondition<T>(s, L, L.r, L.z, levels, st);
-  k_initial_result<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.z, L.S);
-  DT_CUDA(cudaMemcpyAsync(L.p, L.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
-  cudaGraphExec_t exec;
-  DT_TRY(loop_exec<T>(s, L, levels, &exec));
-  DT_CUDA(cudaGraphLaunch(exec, st));
-  return DT_OK;
-}
-
 static dt_status read_scalars(dt_flex* s, const Scalars* S, Scalars* out) {
   DT_CUDA(cudaMemcpyAsync(out, S, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
   DT_CUDA(cudaStreamSynchronize(s->stream));
   return DT_OK;
+}
+
+// host_loop: 0 the device-side graph loop; 1 a host loop with one sync per iteration; 2 the same
+// with each iteration's scalars printed to stderr. Returns with the solve enqueued (graph) or done.
+template <class T>
+static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop) {
+  cudaStream_t st = s->stream;
+  k_begin<<<1, 1, 0, st>>>(L.S); counted();
+  launch_precondition<T>(s, L, L.r, L.z, levels, st);
+  k_initial_result<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.z, L.S); counted();
+  DT_CUDA(cudaMemcpyAsync(L.p, L.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
+  if (!host_loop) {
+    cudaGraphExec_t exec;
+    DT_TRY(loop_exec<T>(s, L, levels, &exec));
+    DT_CUDA(cudaGraphLaunch(exec, st));
+    return DT_OK;
+  }
+  Scalars h;
+  DT_TRY(read_scalars(s, L.S, &h));
+  for (int pass = 0; pass < h.max_it + 2 && h.stop == STOP_RUNNING; ++pass) {
+    launch_iteration<T>(s, L, levels, st);
+    DT_CUDA(cudaGetLastError());
+    DT_TRY(read_scalars(s, L.S, &h));
+    if (host_loop > 1)
+      fprintf(stderr, "pcg(%s) it %d stop %d rr %.6e rz %.6e pap %.6e alpha %.6e beta %.6e err %.6e\n",
+              sizeof(T) == 8 ? "fp64" : "fp32", h.it, h.stop, h.rr, h.rz, h.pap, h.alpha, h.beta, h.err);
+  }
+  return DT_OK;
+}
+
+// Kernels the graph loop ran in its last launch (arm and disarm, and a body per pass).
+template <class T>
+static void count_loop(const Lane<T>& L, int levels, int host_loop, int body_runs) {
+  if (host_loop) return;
+  g_launches += 2 + L.body_kernels[levels == 3 ? 1 : 0] * (long long)body_runs;
 }
 
 // r = b - A x in FP64 with ||r||^2 into S->rr.
@@ -1058,20 +1100,20 @@ static void resid64(dt_flex* s) {
 // ||b||^2 into S->bb
 template <class T>
 static void norm_b(dt_flex* s, const T* b, Scalars* S) {
-  k_dot<T><<<ew_grid(s), 256, 0, s->stream>>>(s->n, b, b, s->partials, S, SITE_DOT);
-  k_take_bb<<<1, 1, 0, s->stream>>>(S);
+  k_dot<T><<<ew_grid(s), 256, 0, s->stream>>>(s->n, b, b, s->partials, S, SITE_DOT); counted();
+  k_take_bb<<<1, 1, 0, s->stream>>>(S); counted();
 }
 
 static dt_status warm_or_cold(dt_flex* s, bool warm) {
   Lane<double>& L = s->L64;
   cudaStream_t st = s->stream;
   if (!warm) {
-    k_fill<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, 0.0);
+    k_fill<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, 0.0); counted();
   }
   resid64(s);  // r = b - A x (r = b for x = 0)
   if (warm) {
-    k_warm_decide<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, L.S);
-    k_warm_record<<<1, 1, 0, st>>>(L.S, s->warm);
+    k_warm_decide<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, L.S); counted();
+    k_warm_record<<<1, 1, 0, st>>>(L.S, s->warm); counted();
   } else {
     WarmInfo none = {0, 1.0};
     DT_CUDA(cudaMemcpyAsync(s->warm, &none, sizeof none, cudaMemcpyHostToDevice, st));
@@ -1088,6 +1130,7 @@ static dt_status fill_report(dt_flex* s, const Scalars& h, int iterations, int r
   rep->refinements = refinements;
   rep->warm_start_accepted = wi.accepted;
   rep->warm_start_rel_residual = wi.rel;
+  rep->kernel_launches = g_launches;
   return DT_OK;
 }
 
@@ -1097,12 +1140,13 @@ static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_r
   cudaStream_t st = s->stream;
   int levels = 1;
   DT_TRY(setup_precond<double>(s, L, p->precond, &levels));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n});
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
   norm_b<double>(s, s->b64, L.S);
   DT_TRY(warm_or_cold(s, warm));
-  DT_TRY(run_pcg<double>(s, L, levels));
+  DT_TRY(run_pcg<double>(s, L, levels, p->host_loop));
   Scalars h;
   DT_TRY(read_scalars(s, L.S, &h));
+  count_loop(L, levels, p->host_loop, h.body_runs);
   int iterations = h.it;
   int stop = h.stop;
   double err = h.err;
@@ -1134,11 +1178,11 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
     set_error("flexure solve: the mixed-precision path stops on a residual rule (DT_STOP_REL_RESIDUAL or DT_STOP_RMS_RESIDUAL)");
     return DT_UNSUPPORTED;
   }
-  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d);
-  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c);
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d); counted();
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
   int levels = 1;
   DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n});
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
   norm_b<double>(s, s->b64, L.S);
   DT_TRY(warm_or_cold(s, warm));
   int iterations = 0, refinements = 0;
@@ -1160,14 +1204,15 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
     }
     if (refinements >= p->max_refinements || iterations >= p->max_iterations) break;
     double itol = std::min(0.5, std::max(p->inner_tol, 0.3 * lim / rel));
-    k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale);
-    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n});
+    k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale); counted();
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
     norm_b<float>(s, F.r, F.S);
-    k_rr_is_bb<<<1, 1, 0, st>>>(F.S);  // x = 0: r = b
-    DT_TRY(run_pcg<float>(s, F, levels));
-    k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale);
+    k_rr_is_bb<<<1, 1, 0, st>>>(F.S); counted();  // x = 0: r = b
+    DT_TRY(run_pcg<float>(s, F, levels, p->host_loop));
+    k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale); counted();
     resid64(s);
     DT_TRY(read_scalars(s, F.S, &hf));
+    count_loop(F, levels, p->host_loop, hf.body_runs);
     iterations += hf.it;
     ++refinements;
     if (hf.stop == STOP_NONFINITE) {
@@ -1222,6 +1267,7 @@ void dt_flex_default_params(dt_flex_params* p) {
   p->max_iterations = 60;  // FlexureParams::default max_iterations (flexure.rs:225)
   p->inner_tol = 1e-5;
   p->max_refinements = 8;
+  p->host_loop = 0;
 }
 
 dt_status dt_flex_destroy(dt_flex* s) {
@@ -1357,8 +1403,10 @@ static dt_status check_params(const dt_flex_params* p) {
 // The solve on inputs already in L64.d, L64.c, b64 (and the guess in L64.x).
 static dt_status solve_loaded(dt_flex* s, const dt_flex_params* p, dt_report* rep) {
   bool warm = p->warm_start != DT_WARM_NONE;
+  long long launches0 = g_launches;
   cudaEventRecord(s->ev0, s->stream);
   dt_status st = p->precision == DT_PREC_MIXED ? solve_mixed(s, p, warm, rep) : solve_fp64(s, p, warm, rep);
+  if (rep) rep->kernel_launches = g_launches - launches0;
   cudaEventRecord(s->ev1, s->stream);
   cudaError_t e = cudaEventSynchronize(s->ev1);
   if (e != cudaSuccess) {
@@ -1445,22 +1493,22 @@ dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, con
   DT_CUDA(cudaMemcpyAsync(L.d, d, bytes, cudaMemcpyHostToDevice, st));
   DT_CUDA(cudaMemcpyAsync(L.c, c, bytes, cudaMemcpyHostToDevice, st));
   DT_CUDA(cudaMemcpyAsync(L.r, r, bytes, cudaMemcpyHostToDevice, st));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n});
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
   if (precision == DT_PREC_MIXED) {
     Lane<float>& F = s->L32;
-    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d);
-    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c);
-    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r);
-    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n});
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d); counted();
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
+    k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r); counted();
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
     int levels;
     DT_TRY(setup_precond<float>(s, F, precond, &levels));
-    k_reset<<<1, 1, 0, st>>>(F.S);
+    k_reset<<<1, 1, 0, st>>>(F.S); counted();
     launch_precondition<float>(s, F, F.r, F.z, levels, st);
-    k_convert<float, double><<<ew_grid(s), 256, 0, st>>>(s->n, F.z, L.z);
+    k_convert<float, double><<<ew_grid(s), 256, 0, st>>>(s->n, F.z, L.z); counted();
   } else {
     int levels;
     DT_TRY(setup_precond<double>(s, L, precond, &levels));
-    k_reset<<<1, 1, 0, st>>>(L.S);
+    k_reset<<<1, 1, 0, st>>>(L.S); counted();
     launch_precondition<double>(s, L, L.r, L.z, levels, st);
   }
   DT_CUDA(cudaGetLastError());
@@ -1470,3 +1518,108 @@ dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, con
 }
 
 }  // extern "C"
+
+// =============================================================================================
+// Kernel timing for the benchmark's roofline: each hot kernel of one PCG iteration launched
+// `reps` times back to back on the handle's stream between two CUDA events, on the handle's
+// current data (after a solve). The CG scalars are reset first with alpha = beta = 0, so the
+// vector updates leave x, r and p as they are.
+
+namespace dt {
+
+__global__ void k_profile_state(Scalars* S) {
+  S->stop = 0;
+  S->started = 1;
+  S->cond = 0ull;
+  S->alpha = 0.0;
+  S->beta = 0.0;
+  S->rz = 1.0;
+  S->it = 0;
+  S->max_it = 1 << 30;
+  S->rule = DT_STOP_MAX_Z;
+  S->tol = -1.0;
+}
+
+template <class T>
+static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, double* bytes) {
+  cudaStream_t st = s->stream;
+  const double e = sizeof(T), n = (double)s->n;
+  // algorithmic bytes per launch: each distinct array read once, each output written once
+  const double algo[DT_PROFILE_KERNELS] = {
+      4 * e * n,  // apply: p, d, c in; Ap out
+      6 * e * n,  // update: x, r, p, Ap in; x, r out
+      3 * e * n,  // direction: z, p in; p out
+      2 * e * n,  // rows forward: r in; half spectrum out (w/2 complex a row = one T a cell)
+      2 * e * n,  // columns: half spectrum in and out
+      3 * e * n,  // rows inverse (with r.z): half spectrum, r in; z out
+      5 * e * n,  // Jacobi left: r, J, d, c in; left out
+      6 * e * n,  // Jacobi final: r, J, part, d, c in; z out
+      3 * e * n,  // rows forward weighted: left, w in; half out
+      4 * e * n,  // rows inverse accumulate: half, w, part in; part out
+  };
+  cudaEvent_t a, b;
+  DT_CUDA(cudaEventCreate(&a));
+  DT_CUDA(cudaEventCreate(&b));
+  for (int k = 0; k < DT_PROFILE_KERNELS; ++k) {
+    k_profile_state<<<1, 1, 0, st>>>(L.S);
+    auto one = [&]() {
+      using C = cplx<T>;
+      int N = s->N, RB = rows_per_block(N);
+      unsigned int rgrid = ceil_div(s->h, RB);
+      int rthreads = RB * N / 8;
+      size_t rsmem = (size_t)RB * N * sizeof(C);
+      int cpb = cols_per_block(s->h, sizeof(C));
+      switch (k) {
+        case 0: launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st); break;
+        case 1: k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); break;
+        case 2: k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); break;
+        case 3: k_rows_fwd<T, false><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.r, nullptr, L.half, L.tab.tw_row, L.tab.post, L.S); break;
+        case 4:
+          k_cols<T><<<ceil_div(N, cpb), cpb * s->h / 8, (size_t)cpb * s->h * sizeof(C), st>>>(
+              N, s->h, L.half, L.tab.tw_col, L.tab.omega, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), L.S, 0);
+          break;
+        case 5:
+          k_rows_inv<T, INV_STORE_DOT><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, L.z, nullptr, L.r, L.tab.tw_row,
+                                                                        L.tab.post, s->partials, L.S);
+          break;
+        case 6: launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, L.r, L.left, L.S, st); break;
+        case 7: launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, L.r, L.z, L.S, st); break;
+        case 8: k_rows_fwd<T, true><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.left, L.wt[0], L.half, L.tab.tw_row, L.tab.post, L.S); break;
+        case 9:
+          k_rows_inv<T, INV_ACCUM><<<rgrid, rthreads, rsmem, st>>>(s->w, s->h, L.half, L.part, L.wt[0], nullptr, L.tab.tw_row,
+                                                                    L.tab.post, s->partials, L.S);
+          break;
+      }
+    };
+    one();  // warm
+    // the precondition finisher may stop the scalars (max|z| < tol never holds with tol < 0)
+    k_profile_state<<<1, 1, 0, st>>>(L.S);
+    DT_CUDA(cudaEventRecord(a, st));
+    for (int r = 0; r < reps; ++r) one();
+    DT_CUDA(cudaEventRecord(b, st));
+    DT_CUDA(cudaEventSynchronize(b));
+    float t = 0.f;
+    DT_CUDA(cudaEventElapsedTime(&t, a, b));
+    ms[k] = (double)t / reps;
+    bytes[k] = algo[k];
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  DT_CUDA(cudaGetLastError());
+  return DT_OK;
+}
+
+}  // namespace dt
+
+extern "C" dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes) {
+  if (!s || !ms || !bytes || reps < 1) {
+    set_error("dt_flex_profile_kernels: bad argument");
+    return DT_BAD_ARG;
+  }
+  dt_status st = precision == DT_PREC_MIXED ? profile_lane<float>(s, s->L32, reps, ms, bytes)
+                                            : profile_lane<double>(s, s->L64, reps, ms, bytes);
+  // leave the scalars of a finished solve stopped
+  k_reset<<<1, 1, 0, s->stream>>>(precision == DT_PREC_MIXED ? s->L32.S : s->L64.S);
+  cudaStreamSynchronize(s->stream);
+  return st;
+}

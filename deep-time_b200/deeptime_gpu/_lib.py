@@ -22,14 +22,15 @@ DIFF_FP64_CG_FP32_CYCLE, DIFF_FP64, DIFF_MIXED = 0, 1, 2
 class FlexParams(ctypes.Structure):
     _fields_ = [("precond", ctypes.c_int), ("stop", ctypes.c_int), ("precision", ctypes.c_int),
                 ("warm_start", ctypes.c_int), ("tol", ctypes.c_double), ("max_iterations", ctypes.c_int),
-                ("inner_tol", ctypes.c_double), ("max_refinements", ctypes.c_int)]
+                ("inner_tol", ctypes.c_double), ("max_refinements", ctypes.c_int),
+                ("host_loop", ctypes.c_int)]
 
 
 class Report(ctypes.Structure):
     _fields_ = [("iterations", ctypes.c_int), ("error_m", ctypes.c_double), ("converged", ctypes.c_int),
                 ("rel_residual", ctypes.c_double), ("refinements", ctypes.c_int),
                 ("warm_start_accepted", ctypes.c_int), ("warm_start_rel_residual", ctypes.c_double),
-                ("device_ms", ctypes.c_double)]
+                ("device_ms", ctypes.c_double), ("kernel_launches", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -63,6 +64,7 @@ def lib():
         L.dt_flex_operator.argtypes = [vp, vp, vp, vp, vp]
         L.dt_flex_bend.argtypes = [vp, vp, vp, vp]
         L.dt_flex_precondition.argtypes = [vp, vp, vp, vp, vp, i, i]
+        L.dt_flex_profile_kernels.argtypes = [vp, i, i, vp, vp]
         _lib = L
     return _lib
 

@@ -31,6 +31,7 @@ class SolveReport:
     warm_start_accepted: bool = False
     warm_start_rel_residual: float = float("nan")
     device_ms: float = float("nan")
+    kernel_launches: int = 0
     status: int = 0
 
 
@@ -43,11 +44,12 @@ def _ptr(a):
 
 
 def params(precond=L.PRECOND_REFERENCE, stop=L.STOP_MAX_Z, precision=L.PREC_FP64, warm_start=L.WARM_NONE, tol=2.0,
-           max_iterations=60, inner_tol=1e-5, max_refinements=8) -> L.FlexParams:
+           max_iterations=60, inner_tol=1e-5, max_refinements=8, host_loop=0) -> L.FlexParams:
     p = L.FlexParams()
     L.lib().dt_flex_default_params(ctypes.byref(p))
     p.precond, p.stop, p.precision, p.warm_start = precond, stop, precision, warm_start
     p.tol, p.max_iterations, p.inner_tol, p.max_refinements = tol, max_iterations, inner_tol, max_refinements
+    p.host_loop = host_loop
     return p
 
 
@@ -95,7 +97,7 @@ class Solver:
         L.check(st, allow=(L.DT_OK, L.DT_NOT_CONVERGED))
         return x.reshape(b.shape), SolveReport(rep.iterations, rep.error_m, bool(rep.converged), rep.rel_residual,
                                                rep.refinements, bool(rep.warm_start_accepted),
-                                               rep.warm_start_rel_residual, rep.device_ms, st)
+                                               rep.warm_start_rel_residual, rep.device_ms, rep.kernel_launches, st)
 
     def operator(self, d, c, v):
         d, c, v = _f64(d), _f64(c), _f64(v)

@@ -65,6 +65,10 @@ typedef struct {
   int max_iterations;   /* PCG iterations (summed over refinements in MIXED) */
   double inner_tol;     /* MIXED: inner relative residual, at least this (default 1e-5) */
   int max_refinements;  /* MIXED: outer FP64 refinements (default 8) */
+  int host_loop;        /* diagnostics: 1 = drive the PCG loop from the host, one sync per
+                           iteration, instead of the device-side graph loop (for profilers that
+                           do not see inside conditional graph nodes); 2 = also print each
+                           iteration's scalars to stderr. Default 0. */
 } dt_flex_params;
 
 typedef struct {
@@ -78,6 +82,7 @@ typedef struct {
   int warm_start_accepted;
   double warm_start_rel_residual; /* ||b - A x0|| / ||b|| of the offered first guess */
   double device_ms;     /* device time of the solve (CUDA events on the handle's stream) */
+  long long kernel_launches; /* this backend's kernels that ran for the solve */
 } dt_report;
 
 typedef struct dt_flex dt_flex;
@@ -103,6 +108,16 @@ dt_status dt_flex_bend(dt_flex* s, const double* d, const double* v, double* y);
 /* z = M^-1 r with the chosen preconditioner (host arrays); for tests of the transforms. */
 dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, const double* r, double* z, int precond,
                                int precision);
+
+/* Benchmark support: the average device time (ms) of each hot kernel of one PCG iteration,
+ * launched `reps` times back to back on the handle's stream between CUDA events, on the
+ * handle's current data (call after a solve; the solve's output was already returned), and each
+ * kernel's algorithmic bytes per launch. Kernel ids, DT_PROFILE_KERNELS of them: 0 operator +
+ * p.Ap, 1 x/r update + r.r, 2 direction, 3 rows forward, 4 column DCT-divide-IDCT, 5 rows
+ * inverse + r.z, 6 Jacobi left, 7 Jacobi final, 8 rows forward weighted, 9 rows inverse
+ * accumulate. `precision` selects the FP64 or the FP32 lane. */
+#define DT_PROFILE_KERNELS 10
+dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes);
 
 const char* dt_last_error(void);
 /* Library and device facts: 1 when a CUDA device is usable, with its name. */
