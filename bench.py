@@ -54,7 +54,25 @@ def parse():
     ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
     ap.add_argument("--precond", default="reference", choices=["reference", "mean_d"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--case", default=None,
+                    help="profiling aid (for ncu): run one host-driven, iteration-capped solve and exit; "
+                         "'W,H,DX,PRECOND,PRECISION,ITERATIONS' with PRECOND 0 reference / 1 mean-D and PRECISION "
+                         "0 fp64 / 1 mixed")
     return ap.parse_args()
+
+
+def run_case(spec):
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import flexure as F
+    from deeptime_gpu import inputs as I
+
+    w, h, dx, pc, prec, its = spec.split(",")
+    w, h, dx, pc, prec, its = int(w), int(h), float(dx), int(pc), int(prec), int(its)
+    d, c, b = I.flexure_problem(w, h, 32.0 if w >= 2048 else 8.0, 1000)
+    sv = F.Solver(w, h, dx)
+    p = F.params(precond=pc, stop=L.STOP_REL_RESIDUAL, precision=prec, tol=TOL, max_iterations=its, host_loop=1)
+    x, rep = sv.solve_with(d, c, b, p)
+    print(rep, flush=True)
 
 
 def dist_init(n):
@@ -206,6 +224,9 @@ def run_reference(args, rank, world):
 
 def main():
     args = parse()
+    if args.case:
+        run_case(args.case)
+        return
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)

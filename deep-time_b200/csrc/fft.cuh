@@ -5,14 +5,26 @@
 // a length-R DFT and writes y[(j/Ns) Ns R + (j mod Ns) + r Ns]; the result is in natural order.
 //
 // Stages run in place through registers: every thread loads its butterflies' inputs, the block
-// synchronises, every thread writes its outputs. A block transforms `batch` sequences of length N
-// stored back to back in shared memory; each thread holds 8 complex values per stage, so the
-// block has batch * N / 8 threads. Twiddles come from a table tw[t] = e^(-2 pi i t / N) built on
-// the host (long double angles); the inverse transform (unnormalised) conjugates them.
+// synchronises, every thread writes its outputs. A block transforms `batch` sequences of length N;
+// each thread holds EPT (8 or 16) complex values per stage, so the block has batch * N / EPT
+// threads. Twiddles come from a table tw[t] = e^(-2 pi i t / N) built on the host (long double
+// angles); the inverse transform (unnormalised) conjugates them.
+//
+// Shared-memory layout: element i of a sequence lives at pad(i) = i + (i >> PADSHIFT), one spare
+// slot after every 16 (8-byte complex) or 8 (16-byte complex) values, i.e. every 128 bytes. The
+// stage's strided writes (stride 8 in the first stage) then fall in distinct banks; a sequence
+// occupies padded_len(N) slots.
 #pragma once
 #include "common.cuh"
 
 namespace dt {
+
+template <class C>
+struct Pad {
+  static constexpr int SHIFT = sizeof(C) == 16 ? 3 : 4;
+  static __host__ __device__ __forceinline__ constexpr int at(int i) { return i + (i >> SHIFT); }
+  static __host__ __device__ __forceinline__ constexpr int len(int n) { return n + (n >> SHIFT) + 1; }
+};
 
 template <class C, bool INV>
 __device__ __forceinline__ void dft2(C& a, C& b) {
@@ -41,7 +53,6 @@ template <class C, bool INV>
 __device__ __forceinline__ void dft8(C* v) {
   using T = decltype(C::x);
   const T h = (T)0.70710678118654752440084436210485;
-  // even and odd halves
   C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
   C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
   dft4<C, INV>(e0, e1, e2, e3);
@@ -60,34 +71,39 @@ __device__ __forceinline__ void dft8(C* v) {
   v[7] = csub(e3, t3);
 }
 
-// One stage of radix R over `batch` sequences of length N in s; span Ns (product of the earlier
-// radices). `tw` has N entries e^(-2 pi i t/N). Threads: batch * N / 8, each owns 8 / R butterflies.
-template <class C, int R, bool INV>
-__device__ __forceinline__ void stockham_stage(C* s, int N, int logN, int Ns, const C* __restrict__ tw) {
-  constexpr int B = 8 / R;  // butterflies per thread
+// One stage of radix R over the block's sequences of length N = 2^LOGN, each stored at
+// s + b * NP (padded); span NS. Everything but the data is known at compile time, so the index
+// arithmetic is shifts and masks. Threads: batch * N / EPT, each owns EPT / R butterflies.
+template <class C, int R, int EPT, bool INV, int LOGN, int NS>
+__device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
+  constexpr int N = 1 << LOGN;
+  constexpr int NP = Pad<C>::len(N);
+  constexpr int B = EPT / R;
+  constexpr int NBF = N / R;
+  constexpr int LOGNBF = LOGN - (R == 8 ? 3 : R == 4 ? 2 : 1);
+  constexpr int STEP = N / (NS * R);
   const int tid = threadIdx.x;
-  const int nbf = N / R;    // butterflies per sequence
   C v[B][R];
-  int outbase[B];
+  int obase[B], oidx[B];
 #pragma unroll
   for (int q = 0; q < B; ++q) {
-    int t = tid * B + q;
-    int b = t / nbf;          // sequence
-    int j = t - b * nbf;      // butterfly within the sequence
-    C* base = s + (size_t)b * N;
-    int k = j & (Ns - 1);
+    int t = tid + q * blockDim.x;
+    int b = t >> LOGNBF;
+    int j = t & (NBF - 1);
+    C* base = s + b * NP;
+    int k = j & (NS - 1);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q][r] = base[j + r * nbf];
-    if (Ns > 1) {
-      int step = (N / (Ns * R)) * k;
+    for (int r = 0; r < R; ++r) v[q][r] = base[Pad<C>::at(j + r * NBF)];
+    if (NS > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        C w = tw[r * step];
+        C w = tw[r * STEP * k];
         if (INV) w.y = -w.y;
         v[q][r] = cmul(v[q][r], w);
       }
     }
-    outbase[q] = b * N + (j - k) * R + k;
+    obase[q] = b * NP;
+    oidx[q] = (j - k) * R + k;
   }
   __syncthreads();
 #pragma unroll
@@ -100,27 +116,31 @@ __device__ __forceinline__ void stockham_stage(C* s, int N, int logN, int Ns, co
       dft2<C, INV>(v[q][0], v[q][1]);
     }
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[outbase[q] + r * Ns] = v[q][r];
+    for (int r = 0; r < R; ++r) s[obase[q] + Pad<C>::at(oidx[q] + r * NS)] = v[q][r];
   }
   __syncthreads();
 }
 
-// Full transform: radix-8 stages, then one radix-4 or radix-2 stage for the remainder.
-// The caller synchronises before (data in s) and may read s after it returns.
-template <class C, bool INV>
-__device__ void smem_fft(C* s, int N, int logN, const C* __restrict__ tw) {
-  int Ns = 1;
-  int rem = logN;
-  while (rem >= 3) {
-    stockham_stage<C, 8, INV>(s, N, logN, Ns, tw);
-    Ns <<= 3;
-    rem -= 3;
+// Stages from span NS on: radix 8 while three or more factors of two remain, then 4 or 2.
+template <class C, int EPT, bool INV, int LOGN, int NS, int REM>
+struct Stages {
+  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
+    if constexpr (REM >= 3) {
+      stockham_stage<C, 8, EPT, INV, LOGN, NS>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 8, REM - 3>::run(s, tw);
+    } else if constexpr (REM == 2) {
+      stockham_stage<C, 4, EPT, INV, LOGN, NS>(s, tw);
+    } else if constexpr (REM == 1) {
+      stockham_stage<C, 2, EPT, INV, LOGN, NS>(s, tw);
+    }
   }
-  if (rem == 2) {
-    stockham_stage<C, 4, INV>(s, N, logN, Ns, tw);
-  } else if (rem == 1) {
-    stockham_stage<C, 2, INV>(s, N, logN, Ns, tw);
-  }
+};
+
+// Full transform of length 2^LOGN. The caller synchronises before (data in s) and may read s
+// after it returns.
+template <class C, int EPT, bool INV, int LOGN>
+__device__ __forceinline__ void smem_fft(C* s, const C* __restrict__ tw) {
+  Stages<C, EPT, INV, LOGN, 1, LOGN>::run(s, tw);
 }
 
 }  // namespace dt
