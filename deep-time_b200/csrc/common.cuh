@@ -25,10 +25,10 @@ const char* last_error();
     }                                                                                        \
   } while (0)
 
-#define DT_TRY(expr)             \
-  do {                           \
-    dt_status s_ = (expr);       \
-    if (s_ != DT_OK) return s_;  \
+#define DT_TRY(...)               \
+  do {                            \
+    dt_status s_ = (__VA_ARGS__); \
+    if (s_ != DT_OK) return s_;   \
   } while (0)
 
 template <class T>
@@ -129,6 +129,46 @@ __device__ __forceinline__ bool last_block(unsigned int* ticket, unsigned int nb
   __syncthreads();
   return is_last;
 }
+
+template <int NV>
+struct Acc {
+  double v[NV];
+};
+
+// Writes this block's partial sums (thread 0 holds them) and, in the last block, reduces all of
+// them in index order. kind: 0 sum, 1 max (per component).
+template <int NV>
+__device__ bool reduce_partials(Acc<NV>& a, const int* kind, double* partials, unsigned int* ticket, unsigned int nblocks) {
+  __shared__ double scratch[32];
+  int tid = threadIdx.x + threadIdx.y * blockDim.x;
+  int nthreads = blockDim.x * blockDim.y;
+  unsigned int bid = blockIdx.x + blockIdx.y * gridDim.x;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double r = kind[q] ? block_max(a.v[q], scratch) : block_sum(a.v[q], scratch);
+    if (tid == 0) partials[(size_t)q * nblocks + bid] = r;
+  }
+  if (!last_block(ticket, nblocks)) return false;
+#pragma unroll
+  for (int q = 0; q < NV; ++q) {
+    double s = kind[q] ? -INFINITY : 0.0;
+    for (unsigned int b = tid; b < nblocks; b += nthreads) {
+      double p = __ldcg(partials + (size_t)q * nblocks + b);
+      s = kind[q] ? fmax(s, p) : s + p;
+    }
+    double r = kind[q] ? block_max(s, scratch) : block_sum(s, scratch);
+    a.v[q] = r;  // valid in thread 0
+  }
+  return true;
+}
+
+// Kernel launches of the calling thread (eager ones, and those recorded while capturing a graph
+// body); defined in flexure.cu.
+void count_launch();
+long long launches_now();
+void add_launches(long long k);
+void begin_capture_count();
+long long end_capture_count();
 
 inline unsigned int ceil_div(size_t a, size_t b) { return (unsigned int)((a + b - 1) / b); }
 inline bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }

@@ -1,0 +1,1256 @@
+// Implicit hillslope/marine diffusion on the B200: (I + dt L_kd) h' = h by conjugate gradients
+// preconditioned with one geometric-multigrid V-cycle.
+//
+// The device implementation behind dt_diff_* (include/deeptime_gpu.h). It solves the system of
+// the reference's diffusion::solve with DiffusionSolver::Multigrid (crates/deeptime-core/src/
+// surface/diffusion.rs:77-110 and surface/diffusion/multigrid.rs:530-763) with its own kernels:
+//
+//   k_d_coeffs     the operator (diffusion.rs:532-603): east/south face couplings
+//                  0.5 (kd_i + kd_j) dt / dx^2 (x wraps when the raster does; 0 on the last row)
+//                  and the diagonal ((((1 + east) + west) + south) + north);
+//   k_d_apply      y = A x in the reference's term order (diag, east, wrap, west, wrap, south,
+//                  north; diffusion.rs:606-650), fused with p.Ap, b - Ax or the mass sums;
+//   multigrid      the levels of multigrid.rs:96-199 (2 x 2 aggregation, coarse couplings SCALE
+//                  times the fine faces crossing, mass the sum) built on the device per solve, and
+//                  two cycles: the reference's (damped Jacobi, omega 0.8, nu 2, to <= 64 cells,
+//                  16 sweeps there; multigrid.rs:243-357, :500-523) and a symmetric multi-colour
+//                  Gauss-Seidel V(2,2) to a 16 x 8 coarsest level (colours forward before the
+//                  coarse correction, backward after it);
+//   CG             multigrid::cg_on's loop (stop on the RMS residual, at most 400 iterations, or
+//                  on the relative residual), then the mass put-back so sum x = sum b
+//                  (multigrid.rs:736-761).
+// The CG loop runs on the device as a CUDA-graph conditional WHILE node, like the flexure solve.
+// Precision: FP64 CG with an FP32 cycle (the reference's split), FP64 throughout, or an FP32
+// inner CG (FP32 cycle) inside FP64 iterative refinement.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dt {
+
+enum { DSITE_PAP = 0, DSITE_UPDATE = 1, DSITE_RZ = 2, DSITE_RESID = 3, DSITE_MASS = 4, DSITE_DOT = 5 };
+enum { DSTOP_RUNNING = 0, DSTOP_CONVERGED = 1, DSTOP_BREAKDOWN = 2, DSTOP_CAP = 3, DSTOP_NONFINITE = 4 };
+
+struct DScalars {
+  double bb, tol;
+  int max_it, rule, n;
+  double rz, pap, alpha, beta, rr, rz_new;
+  int it, stop, body_runs, started;
+  double lost, weight, dot_out;
+  unsigned long long cond;
+  unsigned int ticket[8];
+};
+
+__device__ __forceinline__ void dset_cond(DScalars* S, unsigned int v) {
+  if (S->cond) cudaGraphSetConditional((cudaGraphConditionalHandle)S->cond, v);
+}
+
+__device__ __forceinline__ bool d_converged(const DScalars* S, double rr) {
+  if (S->rule == DT_STOP_REL_RESIDUAL) return rr <= S->tol * S->tol * S->bb;
+  return rr <= S->tol * S->tol * (double)S->n;  // the reference's RMS rule (multigrid.rs:620)
+}
+
+// ---------------------------------------------------------------------------------------------
+// The operator (diffusion.rs:532-650).
+
+__global__ void k_d_coeffs(int w, int h, int wrap, const double* __restrict__ kd, double dt_over_dx2, double* __restrict__ east,
+                           double* __restrict__ south, double* __restrict__ diag, float* __restrict__ east32,
+                           float* __restrict__ south32, float* __restrict__ diag32) {
+  size_t n = (size_t)w * h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % w), j = (int)(k / w);
+    const double* krow = kd + (size_t)j * w;
+    // east face of cell i and of its west neighbour, each as the reference forms it
+    auto face_e = [&](int ii) -> double {
+      if (ii + 1 < w) return 0.5 * (krow[ii] + krow[ii + 1]) * dt_over_dx2;
+      if (wrap) return 0.5 * (krow[ii] + krow[0]) * dt_over_dx2;
+      return 0.0;
+    };
+    auto face_s = [&](int jj) -> double {
+      if (jj + 1 < h) return 0.5 * (kd[(size_t)jj * w + i] + kd[(size_t)(jj + 1) * w + i]) * dt_over_dx2;
+      return 0.0;
+    };
+    double e = face_e(i);
+    double west = i > 0 ? face_e(i - 1) : (wrap ? face_e(w - 1) : 0.0);
+    double s = face_s(j);
+    double north = j > 0 ? face_s(j - 1) : 0.0;
+    double g = 1.0 + e + west + s + north;
+    east[k] = e;
+    south[k] = s;
+    diag[k] = g;
+    east32[k] = (float)e;
+    south32[k] = (float)s;
+    diag32[k] = (float)g;
+  }
+}
+
+// y = A x at cell (i, j): diag, east, (wrap), west, (wrap), south, north (diffusion.rs:614-648).
+template <class T>
+__device__ __forceinline__ T d_apply_at(int w, int h, bool wrap, const T* __restrict__ east, const T* __restrict__ south,
+                                        const T* __restrict__ diag, const T* __restrict__ x, int i, int j) {
+  size_t c = (size_t)j * w + i, c0 = (size_t)j * w;
+  T o = diag[c] * x[c];
+  if (i + 1 < w) o -= east[c] * x[c + 1];
+  if (wrap && i == w - 1) o -= east[c] * x[c0];
+  if (i > 0) o -= east[c - 1] * x[c - 1];
+  if (wrap && i == 0) o -= east[c0 + w - 1] * x[c0 + w - 1];
+  if (j + 1 < h) o -= south[c] * x[c + w];
+  if (j > 0) o -= south[c - w] * x[c - w];
+  return o;
+}
+
+enum { DA_PAP = 0, DA_RESID = 1, DA_MASS = 2, DA_PLAIN = 3 };
+
+// DA_PAP: y = A x, reduce x.y; DA_RESID: y = b - A x, ym = (TM) y, reduce y.y;
+// DA_MASS: reduce sum (b - A x) and sum (diag - 1); DA_PLAIN: y = A x.
+template <class T, class TM, int MODE>
+__global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T* __restrict__ east, const T* __restrict__ south,
+                                                 const T* __restrict__ diag, const T* __restrict__ x, const T* __restrict__ b,
+                                                 T* __restrict__ y, TM* __restrict__ ym, double* partials, DScalars* S) {
+  if (MODE == DA_PAP && S->stop) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) dset_cond(S, 0);
+    return;
+  }
+  size_t n = (size_t)w * h;
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % w), j = (int)(k / w);
+    T ax = d_apply_at<T>(w, h, wrap != 0, east, south, diag, x, i, j);
+    if (MODE == DA_PAP) {
+      y[k] = ax;
+      acc.v[0] += (double)x[k] * (double)ax;
+    } else if (MODE == DA_RESID) {
+      T r = b[k] - ax;
+      y[k] = r;
+      ym[k] = (TM)r;
+      acc.v[0] += (double)r * (double)r;
+    } else if (MODE == DA_MASS) {
+      acc.v[0] += (double)b[k] - (double)ax;
+      acc.v[1] += (double)diag[k] - 1.0;
+    } else {
+      y[k] = ax;
+    }
+  }
+  if (MODE == DA_PLAIN) return;
+  const int kind[2] = {0, 0};
+  int site = MODE == DA_PAP ? DSITE_PAP : MODE == DA_RESID ? DSITE_RESID : DSITE_MASS;
+  if (reduce_partials<2>(acc, kind, partials, &S->ticket[site], gridDim.x) && threadIdx.x == 0) {
+    if (MODE == DA_PAP) {
+      S->pap = acc.v[0];
+      if (!(acc.v[0] > 0.0) || !isfinite(acc.v[0])) {
+        S->stop = isfinite(acc.v[0]) ? DSTOP_BREAKDOWN : DSTOP_NONFINITE;
+        dset_cond(S, 0);
+      } else {
+        S->alpha = S->rz / acc.v[0];
+      }
+    } else if (MODE == DA_RESID) {
+      S->rr = acc.v[0];
+    } else {
+      S->lost = acc.v[0];
+      S->weight = acc.v[1];
+    }
+  }
+}
+
+// x += alpha p; r -= alpha Ap; rm = (TM) r; reduce r.r and test the stopping rule.
+template <class T, class TM>
+__global__ void __launch_bounds__(256) k_d_update(size_t n, T* __restrict__ x, T* __restrict__ r, TM* __restrict__ rm,
+                                                  const T* __restrict__ p, const T* __restrict__ ap, double* partials, DScalars* S) {
+  if (S->stop) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) dset_cond(S, 0);
+    return;
+  }
+  T alpha = (T)S->alpha;
+  Acc<1> acc;
+  acc.v[0] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] += alpha * p[k];
+    T rv = r[k] - alpha * ap[k];
+    r[k] = rv;
+    rm[k] = (TM)rv;
+    acc.v[0] += (double)rv * (double)rv;
+  }
+  const int kind[1] = {0};
+  if (reduce_partials<1>(acc, kind, partials, &S->ticket[DSITE_UPDATE], gridDim.x) && threadIdx.x == 0) {
+    double rr = acc.v[0];
+    S->rr = rr;
+    S->it += 1;
+    if (!isfinite(rr))
+      S->stop = DSTOP_NONFINITE;
+    else if (d_converged(S, rr))
+      S->stop = DSTOP_CONVERGED;
+    else if (S->it >= S->max_it)
+      S->stop = DSTOP_CAP;
+    if (S->stop) dset_cond(S, 0);
+  }
+}
+
+// rz = r . z after the cycle; beta = rz / rz_old (multigrid.rs:721-727).
+template <class T, class TM>
+__global__ void __launch_bounds__(256) k_d_rz(size_t n, const T* __restrict__ r, const TM* __restrict__ z, double* partials,
+                                              DScalars* S) {
+  if (S->stop) return;
+  Acc<1> acc;
+  acc.v[0] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    acc.v[0] += (double)r[k] * (double)z[k];
+  const int kind[1] = {0};
+  if (reduce_partials<1>(acc, kind, partials, &S->ticket[DSITE_RZ], gridDim.x) && threadIdx.x == 0) {
+    double rz = acc.v[0];
+    if (!S->started) {
+      S->started = 1;
+      S->rz = rz;
+      if (!isfinite(rz)) S->stop = DSTOP_NONFINITE;
+      return;
+    }
+    if (!(isfinite(rz) && S->rz > 0.0)) {
+      S->stop = isfinite(rz) ? DSTOP_BREAKDOWN : DSTOP_NONFINITE;
+      dset_cond(S, 0);
+      return;
+    }
+    S->beta = rz / S->rz;
+    S->rz = rz;
+  }
+}
+
+// p = z + beta p (p = z on the first direction), and the loop guard.
+template <class T, class TM>
+__global__ void __launch_bounds__(256) k_d_direction(size_t n, T* __restrict__ p, const TM* __restrict__ z, DScalars* S, int first) {
+  if (!first && blockIdx.x == 0 && threadIdx.x == 0) {
+    int runs = ++S->body_runs;
+    bool again = S->stop == 0 && runs < S->max_it + 2;
+    if (!again && S->stop == 0) S->stop = DSTOP_CAP;
+    dset_cond(S, again ? 1u : 0u);
+  }
+  if (S->stop) return;
+  T beta = first ? (T)0 : (T)S->beta;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    p[k] = first ? (T)z[k] : (T)z[k] + beta * p[k];
+}
+
+// ---------------------------------------------------------------------------------------------
+// The multigrid levels (multigrid.rs:96-199).
+
+template <class TM>
+struct DLevel {
+  int w, h, wrap;
+  TM *east, *south, *diag, *wd, *mass, *r, *z, *t;
+};
+
+template <class TM>
+__global__ void k_mg_finest(size_t n, const double* __restrict__ e, const double* __restrict__ s, const double* __restrict__ g,
+                            TM omega, TM* __restrict__ east, TM* __restrict__ south, TM* __restrict__ diag, TM* __restrict__ wd,
+                            TM* __restrict__ mass) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    east[k] = (TM)e[k];
+    south[k] = (TM)s[k];
+    TM gg = (TM)g[k];
+    diag[k] = gg;
+    wd[k] = omega / gg;
+    mass[k] = (TM)1;
+  }
+}
+
+// Coarse mass and faces: mass = sum of the 2 x 2 block's; east = SCALE * the fine east faces
+// leaving its last column (wrapping), south = SCALE * the fine south faces of its last row.
+template <class TM>
+__global__ void k_mg_coarsen(DLevel<TM> f, DLevel<TM> c, TM scale) {
+  size_t nc = (size_t)c.w * c.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) {
+    int ic = (int)(k % c.w), jc = (int)(k / c.w);
+    int r0 = 2 * jc, r1 = min(2 * jc + 2, f.h), c0 = 2 * ic, c1 = min(2 * ic + 2, f.w);
+    int last_row = r1 - 1, last_col = c1 - 1;
+    TM m = 0;
+    for (int j = r0; j < r1; ++j)
+      for (int i = c0; i < c1; ++i) m += f.mass[(size_t)j * f.w + i];
+    c.mass[k] = m;
+    TM e = 0;
+    if (ic + 1 < c.w || c.wrap) {
+      for (int j = r0; j < r1; ++j) e += f.east[(size_t)j * f.w + last_col];
+      e = scale * e;
+    }
+    c.east[k] = e;
+    TM s = 0;
+    if (jc + 1 < c.h) {
+      for (int i = c0; i < c1; ++i) s += f.south[(size_t)last_row * f.w + i];
+      s = scale * s;
+    }
+    c.south[k] = s;
+  }
+}
+
+template <class TM>
+__global__ void k_mg_diag(DLevel<TM> c, TM omega) {
+  size_t nc = (size_t)c.w * c.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % c.w), j = (int)(k / c.w);
+    size_t c0 = (size_t)j * c.w;
+    TM west = i > 0 ? c.east[k - 1] : (c.wrap ? c.east[c0 + c.w - 1] : (TM)0);
+    TM north = j > 0 ? c.south[k - c.w] : (TM)0;
+    TM g = c.mass[k] + c.east[k] + west + c.south[k] + north;
+    c.diag[k] = g;
+    c.wd[k] = omega / g;
+  }
+}
+
+// A z at a cell of a level, in the level's term order (multigrid.rs:202-240), reading z (+ the
+// coarse correction of each cell's parent when zc is given).
+template <class TM>
+__device__ __forceinline__ TM mg_apply_at(const DLevel<TM>& L, const TM* __restrict__ z, const TM* __restrict__ zc, int wc, int i,
+                                          int j) {
+  auto zat = [&](int ii, int jj) -> TM {
+    TM v = z[(size_t)jj * L.w + ii];
+    if (zc) v += zc[(size_t)(jj / 2) * wc + ii / 2];
+    return v;
+  };
+  size_t c = (size_t)j * L.w + i, c0 = (size_t)j * L.w;
+  TM o = L.diag[c] * zat(i, j);
+  if (i + 1 < L.w) o -= L.east[c] * zat(i + 1, j);
+  if (i > 0) o -= L.east[c - 1] * zat(i - 1, j);
+  if (L.wrap) {
+    if (i == L.w - 1) o -= L.east[c] * zat(0, j);
+    if (i == 0) o -= L.east[c0 + L.w - 1] * zat(L.w - 1, j);
+  }
+  if (j + 1 < L.h) o -= L.south[c] * zat(i, j + 1);
+  if (j > 0) o -= L.south[c - L.w] * zat(i, j - 1);
+  return o;
+}
+
+// z = wd r (the first sweep from z = 0)
+template <class TM>
+__global__ void k_mg_first(DLevel<TM> L, TM* __restrict__ z) {
+  size_t n = (size_t)L.w * L.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) z[k] = L.wd[k] * L.r[k];
+}
+
+// zout = z' + wd (r - A z'), z' = zin (+ the coarse correction)
+template <class TM>
+__global__ void k_mg_sweep(DLevel<TM> L, const TM* __restrict__ zin, TM* __restrict__ zout, const TM* __restrict__ zc, int wc) {
+  size_t n = (size_t)L.w * L.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % L.w), j = (int)(k / L.w);
+    TM zk = zin[k];
+    if (zc) zk += zc[(size_t)(j / 2) * wc + i / 2];
+    TM az = mg_apply_at<TM>(L, zin, zc, wc, i, j);
+    zout[k] = zk + L.wd[k] * (L.r[k] - az);
+  }
+}
+
+// rc = sum over each 2 x 2 block of (r - A z) (multigrid.rs:332-356)
+template <class TM>
+__global__ void k_mg_restrict(DLevel<TM> L, const TM* __restrict__ z, DLevel<TM> C) {
+  size_t nc = (size_t)C.w * C.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) {
+    int ic = (int)(k % C.w), jc = (int)(k / C.w);
+    TM acc = 0;
+    for (int j = 2 * jc; j < min(2 * jc + 2, L.h); ++j)
+      for (int i = 2 * ic; i < min(2 * ic + 2, L.w); ++i) acc += L.r[(size_t)j * L.w + i] - mg_apply_at<TM>(L, z, nullptr, 0, i, j);
+    C.r[k] = acc;
+  }
+}
+
+// The colour of a cell for the Gauss-Seidel sweeps: (i + j) % 2, and on a wrapping level of odd
+// width the last column takes two colours of its own (2 + j % 2), since a ring of odd length has
+// no two-colouring. No two cells of one colour are neighbours.
+__device__ __forceinline__ int gs_colour(int w, int wrap, int i, int j) {
+  if (wrap && (w & 1) && i == w - 1) return 2 + (j & 1);
+  return (i + j) & 1;
+}
+inline int gs_colours(int w, int wrap) { return (wrap && (w & 1)) ? 4 : 2; }
+
+// One Gauss-Seidel pass over the cells of colour `colour`: z_c += (r - A z)_c / diag_c.
+// FIRST: z is taken as 0 where this pass has not written (the cycle's first sweep).
+template <class TM, bool FIRST>
+__global__ void k_mg_gs(DLevel<TM> L, TM* __restrict__ z, int colour) {
+  size_t n = (size_t)L.w * L.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % L.w), j = (int)(k / L.w);
+    int col = gs_colour(L.w, L.wrap, i, j);
+    if (col != colour) continue;
+    // in the first forward sweep, cells of later colours still hold 0 (not yet written)
+    auto zat = [&](int ii, int jj) -> TM {
+      if (FIRST && gs_colour(L.w, L.wrap, ii, jj) >= colour) return (TM)0;
+      return z[(size_t)jj * L.w + ii];
+    };
+    size_t c = k, c0 = (size_t)j * L.w;
+    TM zk = FIRST ? (TM)0 : z[c];
+    TM o = L.diag[c] * zk;
+    if (i + 1 < L.w) o -= L.east[c] * zat(i + 1, j);
+    if (i > 0) o -= L.east[c - 1] * zat(i - 1, j);
+    if (L.wrap) {
+      if (i == L.w - 1) o -= L.east[c] * zat(0, j);
+      if (i == 0) o -= L.east[c0 + L.w - 1] * zat(L.w - 1, j);
+    }
+    if (j + 1 < L.h) o -= L.south[c] * zat(i, j + 1);
+    if (j > 0) o -= L.south[c - L.w] * zat(i, j - 1);
+    z[c] = zk + (L.r[c] - o) / L.diag[c];
+  }
+}
+
+// z += P zc (piecewise constant)
+template <class TM>
+__global__ void k_mg_prolong(DLevel<TM> L, TM* __restrict__ z, const TM* __restrict__ zc, int wc) {
+  size_t n = (size_t)L.w * L.h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % L.w), j = (int)(k / L.w);
+    z[k] += zc[(size_t)(j / 2) * wc + i / 2];
+  }
+}
+
+// The coarsest level in one block (at most 128 cells): KIND 0 the reference's first sweep and
+// 15 damped Jacobi sweeps (multigrid.rs:504-512); KIND 1 eight forward and eight backward
+// multi-colour Gauss-Seidel sweeps. Result in z.
+template <class TM, int KIND>
+__global__ void k_mg_coarsest(DLevel<TM> L, TM* __restrict__ z, int sweeps) {
+  __shared__ TM sz[2][256];
+  int n = L.w * L.h;
+  int k = threadIdx.x;
+  if (KIND == 0) {
+    if (k < n) sz[0][k] = L.wd[k] * L.r[k];
+    __syncthreads();
+    int cur = 0;
+    for (int s = 1; s < sweeps; ++s) {
+      if (k < n) {
+        int i = k % L.w, j = k / L.w;
+        TM az = mg_apply_at<TM>(L, sz[cur], nullptr, 0, i, j);
+        sz[cur ^ 1][k] = sz[cur][k] + L.wd[k] * (L.r[k] - az);
+      }
+      __syncthreads();
+      cur ^= 1;
+    }
+    if (k < n) z[k] = sz[cur][k];
+  } else {
+    if (k < n) sz[0][k] = (TM)0;
+    __syncthreads();
+    int ncol = (L.wrap && (L.w & 1)) ? 4 : 2;
+    for (int pass = 0; pass < 2 * sweeps; ++pass) {
+      bool forward = pass < sweeps;
+      for (int q = 0; q < ncol; ++q) {
+        int colour = forward ? q : ncol - 1 - q;
+        if (k < n) {
+          int i = k % L.w, j = k / L.w;
+          if (gs_colour(L.w, L.wrap, i, j) == colour) {
+            TM az = mg_apply_at<TM>(L, sz[0], nullptr, 0, i, j);
+            sz[0][k] = sz[0][k] + (L.r[k] - az) / L.diag[k];
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (k < n) z[k] = sz[0][k];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// LOD first guess (diffusion.rs:370-489): an implicit sweep along x per row (cyclic tridiagonal,
+// Sherman-Morrison, :1050-1071) and then along y per column (Thomas, :1029-1046). One thread
+// per row or column; scratch arrays of the raster's size.
+
+__device__ void thomas_strided(int n, const double* lo, const double* di, const double* up, double* b, double* c, size_t stride,
+                               size_t base) {
+  // lo/di/up/b/c accessed at base + i * stride
+  if (n == 0) return;
+  double beta = di[base];
+  b[base] /= beta;
+  for (int i = 1; i < n; ++i) {
+    size_t at = base + (size_t)i * stride, prev = at - stride;
+    c[at] = up[prev] / beta;
+    beta = di[at] - lo[at] * c[at];
+    b[at] = (b[at] - lo[at] * b[prev]) / beta;
+  }
+  for (int i = n - 2; i >= 0; --i) {
+    size_t at = base + (size_t)i * stride;
+    double next = b[at + stride];
+    b[at] -= c[at + stride] * next;
+  }
+}
+
+__global__ void k_lod_rows(int w, int h, int wrap, double* __restrict__ hf, const double* __restrict__ kd, double dtdx2,
+                           double* lo, double* di, double* up, double* xs, double* zs, double* cs) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= h) return;
+  size_t c0 = (size_t)j * w;
+  const double* krow = kd + c0;
+  auto face = [&](int i) -> double {
+    if (i + 1 < w) return 0.5 * (krow[i] + krow[i + 1]) * dtdx2;
+    if (wrap && w > 1) return 0.5 * (krow[w - 1] + krow[0]) * dtdx2;
+    return 0.0;
+  };
+  for (int i = 0; i < w; ++i) {
+    double west = i == 0 ? face(w - 1) : face(i - 1);
+    double east = face(i);
+    lo[c0 + i] = -west;
+    up[c0 + i] = -east;
+    di[c0 + i] = 1.0 + west + east;
+  }
+  if (wrap && w > 2) {
+    // cyclic: corners alpha = up[w-1] (row w-1, column 0), beta = lo[0] (row 0, column w-1)
+    double alpha = up[c0 + w - 1], beta = lo[c0];
+    double gamma = -di[c0];
+    di[c0] = di[c0] - gamma;
+    di[c0 + w - 1] = di[c0 + w - 1] - alpha * beta / gamma;
+    lo[c0] = 0.0;
+    up[c0 + w - 1] = 0.0;
+    for (int i = 0; i < w; ++i) {
+      xs[c0 + i] = hf[c0 + i];
+      zs[c0 + i] = 0.0;
+    }
+    zs[c0] = gamma;
+    zs[c0 + w - 1] = alpha;
+    thomas_strided(w, lo, di, up, xs, cs, 1, c0);
+    thomas_strided(w, lo, di, up, zs, cs, 1, c0);
+    double fact = (xs[c0] + beta * xs[c0 + w - 1] / gamma) / (1.0 + zs[c0] + beta * zs[c0 + w - 1] / gamma);
+    for (int i = 0; i < w; ++i) hf[c0 + i] = xs[c0 + i] - fact * zs[c0 + i];
+  } else {
+    if (w == 2 && wrap) {
+      double f = face(0) + face(1);
+      lo[c0 + 1] = -f;
+      up[c0] = -f;
+      di[c0] = 1.0 + f;
+      di[c0 + 1] = 1.0 + f;
+    }
+    lo[c0] = 0.0;
+    up[c0 + w - 1] = 0.0;
+    if (w == 1) di[c0] = 1.0;
+    thomas_strided(w, lo, di, up, hf, cs, 1, c0);
+  }
+}
+
+__global__ void k_lod_cols(int w, int h, double* __restrict__ hf, const double* __restrict__ kd, double dtdx2, double* lo,
+                           double* di, double* up, double* cs) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w) return;
+  auto face = [&](int j) -> double {
+    if (j + 1 < h) return 0.5 * (kd[(size_t)j * w + i] + kd[(size_t)(j + 1) * w + i]) * dtdx2;
+    return 0.0;
+  };
+  for (int j = 0; j < h; ++j) {
+    double north = j == 0 ? 0.0 : face(j - 1);
+    double south = face(j);
+    size_t at = (size_t)j * w + i;
+    lo[at] = -north;
+    up[at] = -south;
+    di[at] = 1.0 + north + south;
+  }
+  thomas_strided(h, lo, di, up, hf, cs, (size_t)w, (size_t)i);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Small control kernels.
+
+__global__ void k_d_arm(DScalars* S, unsigned long long handle) {
+  S->cond = handle;
+  S->body_runs = 0;
+  cudaGraphSetConditional((cudaGraphConditionalHandle)handle, S->stop == 0 ? 1u : 0u);
+}
+__global__ void k_d_disarm(DScalars* S) { S->cond = 0ull; }
+
+struct DProblem {
+  double tol;
+  int max_it, rule, n;
+};
+__global__ void k_d_begin(DScalars* S, DProblem p, int bb_from_dot) {
+  S->tol = p.tol;
+  S->max_it = p.max_it;
+  S->rule = p.rule;
+  S->n = p.n;
+  if (bb_from_dot) S->bb = S->dot_out;
+  S->it = 0;
+  S->stop = 0;
+  S->started = 0;
+  S->body_runs = 0;
+  S->cond = 0ull;
+  if (!isfinite(S->rr) || !isfinite(S->bb))
+    S->stop = DSTOP_NONFINITE;
+  else if (!(S->rr > 0.0) || d_converged(S, S->rr))
+    S->stop = DSTOP_CONVERGED;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_d_dot(size_t n, const T* __restrict__ a, const T* __restrict__ b, double* partials,
+                                               DScalars* S) {
+  Acc<1> acc;
+  acc.v[0] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    acc.v[0] += (double)a[k] * (double)b[k];
+  const int kind[1] = {0};
+  if (reduce_partials<1>(acc, kind, partials, &S->ticket[DSITE_DOT], gridDim.x) && threadIdx.x == 0) S->dot_out = acc.v[0];
+}
+
+// x += (lost / weight)(diag - 1) when weight > 0 and lost != 0 (multigrid.rs:755-761)
+__global__ void k_d_massfix(size_t n, double* __restrict__ x, const double* __restrict__ diag, const DScalars* S) {
+  double lost = S->lost, weight = S->weight;
+  if (!(weight > 0.0 && lost != 0.0)) return;
+  double k = lost / weight;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < n; c += (size_t)gridDim.x * blockDim.x) x[c] += k * (diag[c] - 1.0);
+}
+
+__global__ void k_d_scale_down(size_t n, const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ x32,
+                               const DScalars* S64, double* scale) {
+  double s = S64->rr > 0 ? sqrt((double)n / S64->rr) : 1.0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *scale = s;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    r32[k] = (float)(r[k] * s);
+    x32[k] = 0.0f;
+  }
+}
+__global__ void k_d_accumulate(size_t n, double* __restrict__ x, const float* __restrict__ x32, const double* scale) {
+  double inv = 1.0 / *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += (double)x32[k] * inv;
+}
+__global__ void k_d_rr_is_bb(DScalars* S) { S->rr = S->bb; }
+__global__ void k_convert_dr(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) b[k] = (float)a[k];
+}
+
+}  // namespace dt
+
+// =============================================================================================
+// Host side.
+
+namespace dt {
+
+static const float OMEGA = 0.8f;    // multigrid.rs:45
+static const int NU = 2;            // multigrid.rs:48
+static const float SCALE = 0.5f;    // multigrid.rs:52
+static const int COARSEST = 64;     // multigrid.rs:54
+static const int COARSE_SWEEPS = 16;  // multigrid.rs:56
+static const int COARSEST_GS = 128;   // the Gauss-Seidel cycle's coarsest level: 16 x 8 cells
+static const int COARSE_SWEEPS_GS = 8;
+
+template <class TM>
+struct Hier {
+  std::vector<DLevel<TM>> lv;
+  bool built = false;
+};
+
+// CG lanes: 0 FP64 CG + FP32 cycle, 1 FP64 CG + FP64 cycle, 2 FP32 CG + FP32 cycle (mixed inner)
+struct DGraph {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long body_kernels = 0;
+};
+
+}  // namespace dt
+
+struct dt_diff {
+  int w = 0, h = 0, wrap = 0;
+  double dx = 0;
+  size_t n = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int sms = 148;
+  std::vector<void*> allocs;
+  double *kd = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;
+  double *east = nullptr, *south = nullptr, *diag = nullptr;
+  float *east32 = nullptr, *south32 = nullptr, *diag32 = nullptr;
+  float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
+  double* lod[6] = {};
+  double* partials = nullptr;
+  double* scale = nullptr;
+  dt::DScalars *S64 = nullptr, *S32 = nullptr;
+  dt::Hier<float> hf[2];
+  dt::Hier<double> hd[2];
+  dt::DGraph graph[3][2];
+};
+
+namespace dt {
+
+template <class T>
+static dt_status ddalloc(dt_diff* s, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? DT_OOM : DT_DEVICE_ERROR;
+  }
+  s->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return DT_OK;
+}
+
+static unsigned int dgrid(const dt_diff* s, size_t n) {
+  return std::max(1u, std::min<unsigned int>(ceil_div(n, 256), (unsigned)s->sms * 8));
+}
+
+// The level shapes of the hierarchy (multigrid.rs:117-123): halve (rounding up) until the level
+// has at most `coarsest` cells or stops shrinking; x wraps on a level while it is wider than 1.
+template <class TM>
+static dt_status build_levels(dt_diff* s, Hier<TM>& H, int coarsest) {
+  if (H.built) return DT_OK;
+  int w = s->w, h = s->h, wrap = s->wrap && s->w > 1;
+  for (;;) {
+    DLevel<TM> L;
+    L.w = w;
+    L.h = h;
+    L.wrap = wrap;
+    size_t n = (size_t)w * h;
+    for (TM** q : {&L.east, &L.south, &L.diag, &L.wd, &L.mass, &L.r, &L.z, &L.t}) DT_TRY(ddalloc(s, q, n));
+    H.lv.push_back(L);
+    int wc = (w + 1) / 2, hc = (h + 1) / 2;
+    if ((long)w * h <= coarsest || (wc == w && hc == h)) break;
+    wrap = wrap && wc > 1;
+    w = wc;
+    h = hc;
+  }
+  H.built = true;
+  return DT_OK;
+}
+
+// Level coefficients for the current operator: the finest from the FP64 couplings, the rest by
+// aggregation.
+template <class TM>
+static void fill_levels(dt_diff* s, Hier<TM>& H, cudaStream_t st) {
+  DLevel<TM>& f = H.lv[0];
+  k_mg_finest<TM><<<dgrid(s, s->n), 256, 0, st>>>(s->n, s->east, s->south, s->diag, (TM)OMEGA, f.east, f.south, f.diag, f.wd, f.mass);
+  count_launch();
+  for (size_t l = 1; l < H.lv.size(); ++l) {
+    size_t nc = (size_t)H.lv[l].w * H.lv[l].h;
+    k_mg_coarsen<TM><<<dgrid(s, nc), 256, 0, st>>>(H.lv[l - 1], H.lv[l], (TM)SCALE);
+    k_mg_diag<TM><<<dgrid(s, nc), 256, 0, st>>>(H.lv[l], (TM)OMEGA);
+    count_launch();
+    count_launch();
+  }
+}
+
+// One V-cycle from z = 0 on level l with r set; returns the buffer holding the level's z.
+template <class TM>
+static TM* vcycle(dt_diff* s, Hier<TM>& H, size_t l, int kind, cudaStream_t st) {
+  DLevel<TM>& L = H.lv[l];
+  size_t n = (size_t)L.w * L.h;
+  unsigned int g = dgrid(s, n);
+  bool coarsest = l + 1 == H.lv.size();
+  if (coarsest) {
+    if (kind == DT_CYCLE_JACOBI)
+      k_mg_coarsest<TM, 0><<<1, 256, 0, st>>>(L, L.z, COARSE_SWEEPS);
+    else
+      k_mg_coarsest<TM, 1><<<1, 256, 0, st>>>(L, L.z, COARSE_SWEEPS_GS);
+    count_launch();
+    return L.z;
+  }
+  DLevel<TM>& C = H.lv[l + 1];
+  if (kind == DT_CYCLE_JACOBI) {
+    // multigrid.rs:514-522
+    TM *cur = L.z, *nxt = L.t;
+    k_mg_first<TM><<<g, 256, 0, st>>>(L, cur);
+    count_launch();
+    for (int k = 1; k < NU; ++k) {
+      k_mg_sweep<TM><<<g, 256, 0, st>>>(L, cur, nxt, nullptr, 0);
+      count_launch();
+      std::swap(cur, nxt);
+    }
+    k_mg_restrict<TM><<<dgrid(s, (size_t)C.w * C.h), 256, 0, st>>>(L, cur, C);
+    count_launch();
+    TM* zc = vcycle<TM>(s, H, l + 1, kind, st);
+    k_mg_sweep<TM><<<g, 256, 0, st>>>(L, cur, nxt, zc, C.w);
+    count_launch();
+    std::swap(cur, nxt);
+    for (int k = 1; k < NU; ++k) {
+      k_mg_sweep<TM><<<g, 256, 0, st>>>(L, cur, nxt, nullptr, 0);
+      count_launch();
+      std::swap(cur, nxt);
+    }
+    return cur;
+  }
+  // multi-colour Gauss-Seidel V(NU, NU): colours forward, coarse correction, colours backward
+  int ncol = gs_colours(L.w, L.wrap);
+  for (int sweep = 0; sweep < NU; ++sweep)
+    for (int c = 0; c < ncol; ++c) {
+      if (sweep == 0)
+        k_mg_gs<TM, true><<<g, 256, 0, st>>>(L, L.z, c);
+      else
+        k_mg_gs<TM, false><<<g, 256, 0, st>>>(L, L.z, c);
+      count_launch();
+    }
+  k_mg_restrict<TM><<<dgrid(s, (size_t)C.w * C.h), 256, 0, st>>>(L, L.z, C);
+  count_launch();
+  TM* zc = vcycle<TM>(s, H, l + 1, kind, st);
+  k_mg_prolong<TM><<<g, 256, 0, st>>>(L, L.z, zc, C.w);
+  count_launch();
+  for (int sweep = 0; sweep < NU; ++sweep)
+    for (int c = ncol - 1; c >= 0; --c) {
+      k_mg_gs<TM, false><<<g, 256, 0, st>>>(L, L.z, c);
+      count_launch();
+    }
+  return L.z;
+}
+
+// The CG of one lane: vectors x, r, p, ap in TC; the cycle in TM on the levels of H; rm = H's
+// finest r. Coefficients of the operator in TC.
+template <class TC, class TM>
+struct CgLane {
+  TC *x, *r, *p, *ap, *east, *south, *diag;
+  Hier<TM>* H;
+  DScalars* S;
+  TM* z;  // where the cycle leaves its result (set when the launch sequence is built)
+};
+
+template <class TC, class TM>
+static void cg_iteration(dt_diff* s, CgLane<TC, TM>& C, int kind, cudaStream_t st) {
+  unsigned int g = dgrid(s, s->n);
+  k_d_apply<TC, TM, DA_PAP><<<g, 256, 0, st>>>(s->w, s->h, s->wrap && s->w > 1, C.east, C.south, C.diag, C.p, nullptr, C.ap,
+                                                nullptr, s->partials, C.S);
+  count_launch();
+  k_d_update<TC, TM><<<g, 256, 0, st>>>(s->n, C.x, C.r, C.H->lv[0].r, C.p, C.ap, s->partials, C.S);
+  count_launch();
+  TM* z = vcycle<TM>(s, *C.H, 0, kind, st);
+  C.z = z;
+  k_d_rz<TC, TM><<<g, 256, 0, st>>>(s->n, C.r, z, s->partials, C.S);
+  count_launch();
+  k_d_direction<TC, TM><<<g, 256, 0, st>>>(s->n, C.p, z, C.S, 0);
+  count_launch();
+}
+
+template <class TC, class TM>
+static dt_status cg_graph(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, DGraph** out) {
+  DGraph& G = s->graph[lane][kind];
+  if (G.exec) {
+    *out = &G;
+    return DT_OK;
+  }
+  cudaGraph_t g;
+  DT_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle handle;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+  unsigned long long hv = (unsigned long long)handle;
+  DScalars* Sp = C.S;
+  cudaKernelNodeParams kp = {};
+  void* arm_args[] = {&Sp, &hv};
+  kp.func = (void*)k_d_arm;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(1);
+  kp.kernelParams = arm_args;
+  cudaGraphNode_t n_arm, n_loop, n_disarm;
+  DT_CUDA(cudaGraphAddKernelNode(&n_arm, g, nullptr, 0, &kp));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  begin_capture_count();
+  cg_iteration<TC, TM>(s, C, kind, s->stream);
+  G.body_kernels = end_capture_count();
+  cudaGraph_t captured;
+  DT_CUDA(cudaStreamEndCapture(s->stream, &captured));
+  void* dis_args[] = {&Sp};
+  kp.func = (void*)k_d_disarm;
+  kp.kernelParams = dis_args;
+  DT_CUDA(cudaGraphAddKernelNode(&n_disarm, g, &n_loop, 1, &kp));
+  DT_CUDA(cudaGraphInstantiate(&G.exec, g, 0));
+  G.g = g;
+  *out = &G;
+  return DT_OK;
+}
+
+static dt_status dread(dt_diff* s, const DScalars* S, DScalars* out) {
+  DT_CUDA(cudaMemcpyAsync(out, S, sizeof(DScalars), cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  return DT_OK;
+}
+
+// CG of lane C from x with r = b - A x, rm and S->rr, S->bb already set.
+template <class TC, class TM>
+static dt_status run_cg(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, const DProblem& prob, int host_loop, DScalars* out) {
+  cudaStream_t st = s->stream;
+  unsigned int g = dgrid(s, s->n);
+  k_d_begin<<<1, 1, 0, st>>>(C.S, prob, 0);
+  count_launch();
+  // the first direction: z = M^-1 r, rz, p = z
+  TM* z = vcycle<TM>(s, *C.H, 0, kind, st);
+  k_d_rz<TC, TM><<<g, 256, 0, st>>>(s->n, C.r, z, s->partials, C.S);
+  k_d_direction<TC, TM><<<g, 256, 0, st>>>(s->n, C.p, z, C.S, 1);
+  count_launch();
+  count_launch();
+  if (!host_loop) {
+    DGraph* G;
+    DT_TRY(cg_graph<TC, TM>(s, C, lane, kind, &G));
+    DT_CUDA(cudaGraphLaunch(G->exec, st));
+    DT_TRY(dread(s, C.S, out));
+    add_launches(2 + G->body_kernels * (long long)out->body_runs);
+    return DT_OK;
+  }
+  DT_TRY(dread(s, C.S, out));
+  for (int pass = 0; pass < prob.max_it + 2 && out->stop == DSTOP_RUNNING; ++pass) {
+    cg_iteration<TC, TM>(s, C, kind, st);
+    DT_CUDA(cudaGetLastError());
+    DT_TRY(dread(s, C.S, out));
+    if (host_loop > 1)
+      fprintf(stderr, "diffusion cg it %d stop %d rr %.6e rz %.6e alpha %.6e beta %.6e\n", out->it, out->stop, out->rr, out->rz,
+              out->alpha, out->beta);
+  }
+  return DT_OK;
+}
+
+static dt_status diff_first_guess(dt_diff* s, const dt_diff_params* p, double dt) {
+  cudaStream_t st = s->stream;
+  DT_CUDA(cudaMemcpyAsync(s->x, s->b, s->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  if (p->first_guess) {
+    double dtdx2 = dt / (s->dx * s->dx);
+    k_lod_rows<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, s->wrap, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
+                                                  s->lod[4], s->lod[5]);
+    k_lod_cols<<<ceil_div(s->w, 64), 64, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[5]);
+    count_launch();
+    count_launch();
+  }
+  return DT_OK;
+}
+
+template <class TM>
+static Hier<TM>& hier_for(dt_diff* s, int kind);
+template <>
+Hier<float>& hier_for<float>(dt_diff* s, int kind) {
+  return s->hf[kind];
+}
+template <>
+Hier<double>& hier_for<double>(dt_diff* s, int kind) {
+  return s->hd[kind];
+}
+
+// FP64 CG with a TM cycle (lane 0: TM = float, the reference's split; lane 1: TM = double).
+template <class TM>
+static dt_status solve_fp64_cg(dt_diff* s, const dt_diff_params* p, int lane, dt_report* rep, DScalars* fin) {
+  cudaStream_t st = s->stream;
+  Hier<TM>& H = hier_for<TM>(s, p->cycle);
+  DT_TRY(build_levels<TM>(s, H, p->cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
+  fill_levels<TM>(s, H, st);
+  unsigned int g = dgrid(s, s->n);
+  int wrap = s->wrap && s->w > 1;
+  // bb, then r = b - A x, rm, rr
+  k_d_dot<double><<<g, 256, 0, st>>>(s->n, s->b, s->b, s->partials, s->S64);
+  k_d_begin<<<1, 1, 0, st>>>(s->S64, DProblem{p->tol, p->max_iterations, p->stop, (int)s->n}, 1);
+  k_d_apply<double, TM, DA_RESID><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->x, s->b, s->r, H.lv[0].r,
+                                                     s->partials, s->S64);
+  count_launch();
+  count_launch();
+  count_launch();
+  CgLane<double, TM> C{s->x, s->r, s->p, s->ap, s->east, s->south, s->diag, &H, s->S64, nullptr};
+  DT_TRY(run_cg<double, TM>(s, C, lane, p->cycle, DProblem{p->tol, p->max_iterations, p->stop, (int)s->n}, p->host_loop, fin));
+  if (rep) rep->iterations = fin->it;
+  return DT_OK;
+}
+
+// FP32 inner CG (FP32 cycle) inside FP64 refinement on the residual scaled to unit RMS.
+static dt_status solve_mixed_cg(dt_diff* s, const dt_diff_params* p, dt_report* rep, DScalars* fin) {
+  cudaStream_t st = s->stream;
+  Hier<float>& H = s->hf[p->cycle];
+  DT_TRY(build_levels<float>(s, H, p->cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
+  fill_levels<float>(s, H, st);
+  unsigned int g = dgrid(s, s->n);
+  int wrap = s->wrap && s->w > 1;
+  k_d_dot<double><<<g, 256, 0, st>>>(s->n, s->b, s->b, s->partials, s->S64);
+  k_d_begin<<<1, 1, 0, st>>>(s->S64, DProblem{p->tol, p->max_iterations, p->stop, (int)s->n}, 1);
+  count_launch();
+  count_launch();
+  int iterations = 0, refinements = 0;
+  DScalars h64, h32;
+  h32.stop = DSTOP_RUNNING;
+  bool nonfinite = false;
+  for (;;) {
+    k_d_apply<double, float, DA_RESID><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->x, s->b, s->r, s->r32,
+                                                          s->partials, s->S64);
+    count_launch();
+    DT_TRY(dread(s, s->S64, &h64));
+    if (!std::isfinite(h64.rr) || !std::isfinite(h64.bb)) {
+      nonfinite = true;
+      break;
+    }
+    double lim2 = p->stop == DT_STOP_REL_RESIDUAL ? p->tol * p->tol * h64.bb : p->tol * p->tol * (double)s->n;
+    if (h64.rr <= lim2) break;
+    if (refinements >= p->max_refinements || iterations >= p->max_iterations) break;
+    double rel = std::sqrt(h64.rr / std::max(lim2, 1e-300));  // > 1: how far above the target
+    double itol = std::min(0.5, std::max(p->inner_tol, 0.3 / rel));
+    k_d_scale_down<<<g, 256, 0, st>>>(s->n, s->r, s->r32, s->x32, s->S64, s->scale);
+    // the inner system's b is the scaled residual: bb = its r.r, x = 0
+    k_d_dot<float><<<g, 256, 0, st>>>(s->n, s->r32, s->r32, s->partials, s->S32);
+    k_d_begin<<<1, 1, 0, st>>>(s->S32, DProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n}, 1);
+    k_d_rr_is_bb<<<1, 1, 0, st>>>(s->S32);
+    // the cycle's finest rhs is the inner CG's r in FP32
+    cudaMemcpyAsync(H.lv[0].r, s->r32, s->n * sizeof(float), cudaMemcpyDeviceToDevice, st);
+    count_launch();
+    count_launch();
+    count_launch();
+    count_launch();
+    CgLane<float, float> C{s->x32, s->r32, s->p32, s->ap32, s->east32, s->south32, s->diag32, &H, s->S32, nullptr};
+    DT_TRY(run_cg<float, float>(s, C, 2, p->cycle, DProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n},
+                                p->host_loop, &h32));
+    k_d_accumulate<<<g, 256, 0, st>>>(s->n, s->x, s->x32, s->scale);
+    count_launch();
+    iterations += h32.it;
+    ++refinements;
+    if (h32.stop == DSTOP_NONFINITE) {
+      nonfinite = true;
+      break;
+    }
+  }
+  *fin = h64;
+  fin->it = iterations;
+  fin->stop = nonfinite ? DSTOP_NONFINITE
+                        : (h64.rr <= (p->stop == DT_STOP_REL_RESIDUAL ? p->tol * p->tol * h64.bb : p->tol * p->tol * (double)s->n)
+                               ? DSTOP_CONVERGED
+                               : DSTOP_CAP);
+  if (rep) {
+    rep->iterations = iterations;
+    rep->refinements = refinements;
+  }
+  return DT_OK;
+}
+
+}  // namespace dt
+
+using namespace dt;
+
+extern "C" {
+
+void dt_diff_default_params(dt_diff_params* p) {
+  if (!p) return;
+  p->cycle = DT_CYCLE_JACOBI;
+  p->precision = DT_DIFF_FP64_CG_FP32_CYCLE;
+  p->stop = DT_STOP_RMS_RESIDUAL;
+  p->tol = 1e-5;             // surface.numerics.diffusion_tol_m (params.rs:197-200)
+  p->max_iterations = 400;   // CG_MAX_ITER (diffusion.rs:497)
+  p->first_guess = 1;        // the LOD splitting (diffusion.rs:101-110)
+  p->inner_tol = 1e-5;
+  p->max_refinements = 8;
+  p->host_loop = 0;
+}
+
+dt_status dt_diff_destroy(dt_diff* s) {
+  if (!s) return DT_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (auto& a : s->graph)
+    for (auto& G : a) {
+      if (G.exec) cudaGraphExecDestroy(G.exec);
+      if (G.g) cudaGraphDestroy(G.g);
+    }
+  for (void* q : s->allocs) cudaFree(q);
+  if (s->ev0) cudaEventDestroy(s->ev0);
+  if (s->ev1) cudaEventDestroy(s->ev1);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return DT_OK;
+}
+
+dt_status dt_diff_create(int w, int h, double dx, int wrap_x, dt_diff** out) {
+  if (!out) {
+    set_error("dt_diff_create: out is NULL");
+    return DT_BAD_ARG;
+  }
+  *out = nullptr;
+  if (w < 1 || h < 1 || !(dx > 0.0) || !std::isfinite(dx)) {
+    set_error("dt_diff_create: bad raster %d x %d, dx %g", w, h, dx);
+    return DT_BAD_ARG;
+  }
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    set_error("dt_diff_create: no CUDA device");
+    return DT_DEVICE_ERROR;
+  }
+  auto* s = new dt_diff();
+  s->w = w;
+  s->h = h;
+  s->dx = dx;
+  s->wrap = wrap_x ? 1 : 0;
+  s->n = (size_t)w * h;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, 0) == cudaSuccess) s->sms = prop.multiProcessorCount;
+  auto fail = [&](dt_status e) {
+    dt_diff_destroy(s);
+    return e;
+  };
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(DT_DEVICE_ERROR);
+  s->own_stream = true;
+  dt_status st;
+  for (double** q : {&s->kd, &s->b, &s->x, &s->r, &s->p, &s->ap, &s->east, &s->south, &s->diag})
+    if ((st = ddalloc(s, q, s->n)) != DT_OK) return fail(st);
+  for (float** q : {&s->east32, &s->south32, &s->diag32, &s->x32, &s->r32, &s->p32, &s->ap32})
+    if ((st = ddalloc(s, q, s->n)) != DT_OK) return fail(st);
+  for (int k = 0; k < 6; ++k)
+    if ((st = ddalloc(s, &s->lod[k], s->n)) != DT_OK) return fail(st);
+  if ((st = ddalloc(s, &s->partials, (size_t)s->sms * 8 * 2)) != DT_OK) return fail(st);
+  if ((st = ddalloc(s, &s->scale, 1)) != DT_OK) return fail(st);
+  if ((st = ddalloc(s, &s->S64, 1)) != DT_OK) return fail(st);
+  if ((st = ddalloc(s, &s->S32, 1)) != DT_OK) return fail(st);
+  cudaMemset(s->S64, 0, sizeof(DScalars));
+  cudaMemset(s->S32, 0, sizeof(DScalars));
+  if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) return fail(DT_DEVICE_ERROR);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_error("dt_diff_create: %s", cudaGetErrorString(e));
+    return fail(DT_DEVICE_ERROR);
+  }
+  *out = s;
+  return DT_OK;
+}
+
+dt_status dt_diff_set_stream(dt_diff* s, void* stream) {
+  if (!s) return DT_BAD_ARG;
+  cudaStreamSynchronize(s->stream);
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  if (stream) {
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) return DT_DEVICE_ERROR;
+    s->own_stream = true;
+  }
+  return DT_OK;
+}
+
+static dt_status diff_check(const dt_diff_params* p, double dt) {
+  if (!p) {
+    set_error("diffusion solve: params is NULL");
+    return DT_BAD_ARG;
+  }
+  if ((p->cycle != DT_CYCLE_JACOBI && p->cycle != DT_CYCLE_RBGS) || p->precision < 0 || p->precision > 2 ||
+      (p->stop != DT_STOP_RMS_RESIDUAL && p->stop != DT_STOP_REL_RESIDUAL) || !(p->tol >= 0.0) || p->max_iterations < 0) {
+    set_error("diffusion solve: bad parameters (cycle %d, precision %d, rule %d, tol %g)", p->cycle, p->precision, p->stop, p->tol);
+    return DT_BAD_ARG;
+  }
+  if (!(dt > 0.0) || !std::isfinite(dt)) {
+    set_error("diffusion solve: dt must be positive and finite (got %g)", dt);
+    return DT_BAD_ARG;
+  }
+  return DT_OK;
+}
+
+// The solve on kd and b already on the device (the handle's buffers).
+static dt_status diff_solve_loaded(dt_diff* s, double dt, const dt_diff_params* p, dt_report* rep) {
+  cudaStream_t st = s->stream;
+  long long l0 = launches_now();
+  cudaEventRecord(s->ev0, st);
+  double dtdx2 = dt / (s->dx * s->dx);
+  k_d_coeffs<<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, s->wrap && s->w > 1, s->kd, dtdx2, s->east, s->south, s->diag, s->east32,
+                                             s->south32, s->diag32);
+  count_launch();
+  DT_TRY(diff_first_guess(s, p, dt));
+  DScalars fin;
+  memset(&fin, 0, sizeof fin);
+  if (rep) memset(rep, 0, sizeof *rep);
+  if (p->precision == DT_DIFF_MIXED) {
+    DT_TRY(solve_mixed_cg(s, p, rep, &fin));
+  } else if (p->precision == DT_DIFF_FP64) {
+    DT_TRY(solve_fp64_cg<double>(s, p, 1, rep, &fin));
+  } else {
+    DT_TRY(solve_fp64_cg<float>(s, p, 0, rep, &fin));
+  }
+  // mass put-back: sum x = sum b (multigrid.rs:736-761)
+  unsigned int g = dgrid(s, s->n);
+  int wrap = s->wrap && s->w > 1;
+  k_d_apply<double, float, DA_MASS><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->x, s->b, nullptr, nullptr,
+                                                       s->partials, s->S64);
+  k_d_massfix<<<g, 256, 0, st>>>(s->n, s->x, s->diag, s->S64);
+  // the answer's relative residual
+  k_d_apply<double, float, DA_RESID><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->x, s->b, s->ap, s->r32,
+                                                        s->partials, s->S64);
+  count_launch();
+  count_launch();
+  count_launch();
+  cudaEventRecord(s->ev1, st);
+  DScalars h;
+  DT_TRY(dread(s, s->S64, &h));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  if (rep) {
+    rep->converged = fin.stop == DSTOP_CONVERGED;
+    rep->rel_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
+    rep->error_m = std::sqrt(h.rr / (double)s->n);  // the RMS residual, m
+    rep->device_ms = ms;
+    rep->kernel_launches = launches_now() - l0;
+  }
+  if (fin.stop == DSTOP_NONFINITE || !std::isfinite(h.rr)) {
+    set_error("diffusion solve: a non-finite value appeared");
+    return DT_NONFINITE;
+  }
+  return fin.stop == DSTOP_CONVERGED ? DT_OK : DT_NOT_CONVERGED;
+}
+
+dt_status dt_diff_solve(dt_diff* s, double* h_inout, const double* kd, double dt, const dt_diff_params* p, dt_report* rep) {
+  if (!s || !h_inout || !kd) {
+    set_error("dt_diff_solve: NULL argument");
+    return DT_BAD_ARG;
+  }
+  DT_TRY(diff_check(p, dt));
+  size_t bytes = s->n * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->b, h_inout, bytes, cudaMemcpyHostToDevice, s->stream));
+  dt_status st = diff_solve_loaded(s, dt, p, rep);
+  if (st == DT_OK || st == DT_NOT_CONVERGED) {
+    DT_CUDA(cudaMemcpyAsync(h_inout, s->x, bytes, cudaMemcpyDeviceToHost, s->stream));
+    DT_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
+}
+
+dt_status dt_diff_solve_dev(dt_diff* s, double* h_inout, const double* kd, double dt, const dt_diff_params* p, dt_report* rep) {
+  if (!s || !h_inout || !kd) {
+    set_error("dt_diff_solve_dev: NULL argument");
+    return DT_BAD_ARG;
+  }
+  DT_TRY(diff_check(p, dt));
+  size_t bytes = s->n * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->b, h_inout, bytes, cudaMemcpyDeviceToDevice, s->stream));
+  dt_status st = diff_solve_loaded(s, dt, p, rep);
+  if (st == DT_OK || st == DT_NOT_CONVERGED) {
+    DT_CUDA(cudaMemcpyAsync(h_inout, s->x, bytes, cudaMemcpyDeviceToDevice, s->stream));
+    DT_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  return st;
+}
+
+dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double* x, double* y) {
+  if (!s || !kd || !x || !y) {
+    set_error("dt_diff_operator: NULL argument");
+    return DT_BAD_ARG;
+  }
+  size_t bytes = s->n * sizeof(double);
+  cudaStream_t st = s->stream;
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, st));
+  DT_CUDA(cudaMemcpyAsync(s->p, x, bytes, cudaMemcpyHostToDevice, st));
+  int wrap = s->wrap && s->w > 1;
+  k_d_coeffs<<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, wrap, s->kd, dt / (s->dx * s->dx), s->east, s->south, s->diag, s->east32,
+                                             s->south32, s->diag32);
+  k_d_apply<double, float, DA_PLAIN><<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->p, nullptr,
+                                                                    s->ap, nullptr, s->partials, s->S64);
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(y, s->ap, bytes, cudaMemcpyDeviceToHost, st));
+  DT_CUDA(cudaStreamSynchronize(st));
+  return DT_OK;
+}
+
+dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, const double* r, float* z, int* levels) {
+  if (!s || !kd || !r || !z || (cycle != DT_CYCLE_JACOBI && cycle != DT_CYCLE_RBGS)) {
+    set_error("dt_diff_vcycle: bad argument");
+    return DT_BAD_ARG;
+  }
+  size_t bytes = s->n * sizeof(double);
+  cudaStream_t st = s->stream;
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, st));
+  DT_CUDA(cudaMemcpyAsync(s->r, r, bytes, cudaMemcpyHostToDevice, st));
+  int wrap = s->wrap && s->w > 1;
+  k_d_coeffs<<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, wrap, s->kd, dt / (s->dx * s->dx), s->east, s->south, s->diag, s->east32,
+                                             s->south32, s->diag32);
+  Hier<float>& H = s->hf[cycle];
+  DT_TRY(build_levels<float>(s, H, cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
+  fill_levels<float>(s, H, st);
+  k_convert_dr<<<dgrid(s, s->n), 256, 0, st>>>(s->n, s->r, H.lv[0].r);
+  float* zz = vcycle<float>(s, H, 0, cycle, st);
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(z, zz, s->n * sizeof(float), cudaMemcpyDeviceToHost, st));
+  DT_CUDA(cudaStreamSynchronize(st));
+  if (levels) *levels = (int)H.lv.size();
+  return DT_OK;
+}
+
+}  // extern "C"

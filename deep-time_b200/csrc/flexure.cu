@@ -169,38 +169,6 @@ __device__ void finish_stats(Scalars* S, double lo, double hi, double sum_c, dou
 // ---------------------------------------------------------------------------------------------
 // Reduction epilogue shared by the kernels: block partials -> last block -> finisher.
 
-template <int NV>
-struct Acc {
-  double v[NV];
-};
-
-// Writes this block's partial sums (thread 0 holds them) and, in the last block, reduces all of
-// them in index order. kind: 0 sum, 1 max (per component).
-template <int NV>
-__device__ bool reduce_partials(Acc<NV>& a, const int* kind, double* partials, unsigned int* ticket, unsigned int nblocks) {
-  __shared__ double scratch[32];
-  int tid = threadIdx.x + threadIdx.y * blockDim.x;
-  int nthreads = blockDim.x * blockDim.y;
-  unsigned int bid = blockIdx.x + blockIdx.y * gridDim.x;
-#pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double r = kind[q] ? block_max(a.v[q], scratch) : block_sum(a.v[q], scratch);
-    if (tid == 0) partials[(size_t)q * nblocks + bid] = r;
-  }
-  if (!last_block(ticket, nblocks)) return false;
-#pragma unroll
-  for (int q = 0; q < NV; ++q) {
-    double s = kind[q] ? -INFINITY : 0.0;
-    for (unsigned int b = tid; b < nblocks; b += nthreads) {
-      double p = __ldcg(partials + (size_t)q * nblocks + b);
-      s = kind[q] ? fmax(s, p) : s + p;
-    }
-    double r = kind[q] ? block_max(s, scratch) : block_sum(s, scratch);
-    a.v[q] = r;  // valid in thread 0
-  }
-  return true;
-}
-
 // ---------------------------------------------------------------------------------------------
 // The 13-point operator over a tile.
 
@@ -496,6 +464,9 @@ __global__ void __launch_bounds__(256) k_bank_weights(int w, int h, const T* __r
 // FFT stage, so a block of `batch` sequences of length L has batch * L / FFT_EPT threads.
 
 enum { INV_STORE = 0, INV_ACCUM = 1, INV_STORE_DOT = 2, INV_STORE_W = 3 };
+// Correctly rounded reciprocals (double: one division; float: the intrinsic).
+__device__ __forceinline__ double recip(double x) { return 1.0 / x; }
+__device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 constexpr int FFT_EPT = 16;
 constexpr int FFT_MAX_THREADS = 512;
 
@@ -512,7 +483,7 @@ __host__ __device__ constexpr int cols_per_block(int logh, int elem) {
 }
 
 template <class T, bool WEIGHT, int LOGN>
-__global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_fwd(int w, int h, const T* __restrict__ v, const T* __restrict__ wt,
+__global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_rows_fwd(int w, int h, const T* __restrict__ v, const T* __restrict__ wt,
                                                              cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
                                                              const cplx<T>* __restrict__ post, const Scalars* S) {
   using C = cplx<T>;
@@ -526,6 +497,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_fwd(int w, int h, cons
   const int row0 = blockIdx.x * RB;
   const int tid = threadIdx.x;
   // load rows as complex pairs (v[2n], v[2n+1]): one 2-wide vector load per pair
+#pragma unroll 1
   for (int idx = tid; idx < RB * N; idx += blockDim.x) {
     int rb = idx >> logN, nn = idx & (N - 1);
     int j = row0 + rb;
@@ -545,6 +517,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_fwd(int w, int h, cons
   smem_fft<C, FFT_EPT, false, LOGN>(s, tw);
   // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
   constexpr int half_n = N / 2 + 1;
+#pragma unroll 1
   for (int idx = tid; idx < RB * half_n; idx += blockDim.x) {
     int rb = idx / half_n, kk = idx - rb * half_n;
     int j = row0 + rb;
@@ -568,7 +541,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_fwd(int w, int h, cons
 // The column pass: DCT-II along y (Makhoul), divide by d lambda^2 + c_ref, inverse DCT.
 // lx[k] = 2 cos(2 pi k / w) - 2 for k = 0..N; ly[m] = 2 cos(pi m / h) - 2.
 template <class T, int LOGH>
-__global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
+__global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_cols(int N, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
                                                          const cplx<T>* __restrict__ omega, const T* __restrict__ lx,
                                                          const T* __restrict__ ly, T inv_dx2, const Scalars* S, int level) {
   using C = cplx<T>;
@@ -584,6 +557,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __rest
   const int tid = threadIdx.x;
   const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
   // gather with the even-first / odd-reversed order (consecutive threads: consecutive columns)
+#pragma unroll 1
   for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
     int j = idx >> logc, cc = idx & (CPB - 1);
     int k = k0 + cc;
@@ -595,25 +569,27 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __rest
   smem_fft<C, FFT_EPT, false, LOGH>(s, tw);
   // per column and pair (m, h - m): C[m] = (w_m V[m] + i w_(h-m) V[h-m]) / 2, divide, and back
   constexpr int half_h = h / 2 + 1;
+#pragma unroll 1
   for (int idx = tid; idx < CPB * half_h; idx += blockDim.x) {
     int cc = idx / half_h, m = idx - cc * half_h;
     int k = k0 + cc;
     if (k >= N) continue;
     C* col = s + cc * HP;
     // divisors: column 0 is packed (real part k = 0, imaginary part k = N)
-    auto den = [&](int kx, int mm) {
+    // 1 / (d lambda^2 + c): one reciprocal per divisor, then products
+    auto rden = [&](int kx, int mm) {
       T l = (lx[kx] + ly[mm]) * inv_dx2;
-      return dref * (l * l) + cref;
+      return recip(dref * (l * l) + cref);
     };
     if (m == 0) {
       C v0 = col[0];
       if (k == 0) {
-        v0.x /= den(0, 0);
-        v0.y /= den(N, 0);
+        v0.x *= rden(0, 0);
+        v0.y *= rden(N, 0);
       } else {
-        T dd = den(k, 0);
-        v0.x /= dd;
-        v0.y /= dd;
+        T dd = rden(k, 0);
+        v0.x *= dd;
+        v0.y *= dd;
       }
       col[0] = v0;
       continue;
@@ -625,16 +601,16 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __rest
     C cm = cscale(cadd(p, cmuli(q)), (T)0.5);
     C cn = cscale(cadd(q, cmuli(p)), (T)0.5);
     if (k == 0) {
-      cm.x /= den(0, m);
-      cm.y /= den(N, m);
-      cn.x /= den(0, mm);
-      cn.y /= den(N, mm);
+      cm.x *= rden(0, m);
+      cm.y *= rden(N, m);
+      cn.x *= rden(0, mm);
+      cn.y *= rden(N, mm);
     } else {
-      T a = den(k, m), b = den(k, mm);
-      cm.x /= a;
-      cm.y /= a;
-      cn.x /= b;
-      cn.y /= b;
+      T a = rden(k, m), b = rden(k, mm);
+      cm.x *= a;
+      cm.y *= a;
+      cn.x *= b;
+      cn.y *= b;
     }
     // V'[m] = conj(w_m) (C[m] - i C[h-m])
     C vm = cmul(cconj(omega[m]), csub(cm, cmuli(cn)));
@@ -643,8 +619,13 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __rest
     if (mm != m) col[pn] = vn;
   }
   __syncthreads();
-  smem_fft<C, FFT_EPT, true, LOGH>(s, tw);
+  // the same table through a pointer the compiler cannot prove equal to `tw`: otherwise it keeps
+  // the forward stages' twiddles in registers for the inverse stages and spills
+  const C* tw_inv;
+  asm volatile("mov.b64 %0, %1;" : "=l"(tw_inv) : "l"(tw));
+  smem_fft<C, FFT_EPT, true, LOGH>(s, tw_inv);
   const T inv_h = (T)1 / (T)h;
+#pragma unroll 1
   for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
     int j = idx >> logc, cc = idx & (CPB - 1);
     int k = k0 + cc;
@@ -657,7 +638,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_cols(int N, cplx<T>* __rest
 // Inverse rows: Z[k] = E[k] + i O[k] with E = (X[k] + conj X[N-k]) / 2,
 // O = (X[k] - conj X[N-k]) conj(W^k) / 2; x = IFFT_N(Z) / N de-interleaved.
 template <class T, int MODE, int LOGN>
-__global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_inv(int w, int h, const cplx<T>* __restrict__ half, T* __restrict__ out,
+__global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_rows_inv(int w, int h, const cplx<T>* __restrict__ half, T* __restrict__ out,
                                                              const T* __restrict__ wt, const T* __restrict__ r,
                                                              const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ post,
                                                              double* partials, Scalars* S) {
@@ -675,6 +656,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_inv(int w, int h, cons
   const int row0 = blockIdx.x * RB;
   const int tid = threadIdx.x;
   constexpr int half_n = N / 2 + 1;
+#pragma unroll 1
   for (int idx = tid; idx < RB * half_n; idx += blockDim.x) {
     int rb = idx / half_n, kk = idx - rb * half_n;
     int j = row0 + rb;
@@ -707,6 +689,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS) k_rows_inv(int w, int h, cons
   Acc<2> acc;
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
+#pragma unroll 1
   for (int idx = tid; idx < RB * N; idx += blockDim.x) {
     int rb = idx >> logN, nn = idx & (N - 1);
     int j = row0 + rb;
@@ -830,6 +813,17 @@ static inline void counted() {
     ++g_captured;
   else
     ++g_launches;
+}
+void count_launch() { counted(); }
+long long launches_now() { return g_launches; }
+void add_launches(long long k) { g_launches += k; }
+void begin_capture_count() {
+  g_capturing = true;
+  g_captured = 0;
+}
+long long end_capture_count() {
+  g_capturing = false;
+  return g_captured;
 }
 
 template <class T>

@@ -109,6 +109,36 @@ dt_status dt_flex_bend(dt_flex* s, const double* d, const double* v, double* y);
 dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, const double* r, double* z, int precond,
                                int precision);
 
+/* ---- diffusion ------------------------------------------------------------------------------ */
+
+typedef struct {
+  int cycle;            /* DT_CYCLE_JACOBI (the reference's, default) or DT_CYCLE_RBGS */
+  int precision;        /* DT_DIFF_FP64_CG_FP32_CYCLE (the reference's, default), DT_DIFF_FP64, DT_DIFF_MIXED */
+  int stop;             /* DT_STOP_RMS_RESIDUAL (the reference's: RMS residual < tol metres) or DT_STOP_REL_RESIDUAL */
+  double tol;           /* default 1e-5 m (surface.numerics.diffusion_tol_m, params.rs:197-200) */
+  int max_iterations;   /* default 400 (CG_MAX_ITER, diffusion.rs:497) */
+  int first_guess;      /* 1: the LOD splitting's first guess (the reference, diffusion.rs:101-110); 0: h itself */
+  double inner_tol;     /* MIXED: inner relative residual, at least this (default 1e-5) */
+  int max_refinements;  /* MIXED: outer FP64 refinements (default 8) */
+  int host_loop;        /* diagnostics, as dt_flex_params.host_loop */
+} dt_diff_params;
+
+void dt_diff_default_params(dt_diff_params* p);
+/* A w x h raster of dx metres, x wrapping when wrap_x (Dims, crates/deeptime-core/src/surface/grid.rs:11-17). */
+dt_status dt_diff_create(int w, int h, double dx, int wrap_x, dt_diff** out);
+dt_status dt_diff_destroy(dt_diff* s);
+dt_status dt_diff_set_stream(dt_diff* s, void* stream);
+/* One implicit step: h_inout holds h (m) on entry and h' on return; kd the diffusivity per cell
+ * (m^2/yr), dt the step (yr). Iterations in rep->iterations (diffusion::solve's return value);
+ * rep->error_m is the final RMS residual (m). */
+dt_status dt_diff_solve(dt_diff* s, double* h_inout, const double* kd, double dt, const dt_diff_params* p, dt_report* rep);
+dt_status dt_diff_solve_dev(dt_diff* s, double* h_inout, const double* kd, double dt, const dt_diff_params* p, dt_report* rep);
+/* y = (I + dt L_kd) x (host arrays). */
+dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double* x, double* y);
+/* z = M^-1 r, one V-cycle from z = 0 (FP32 levels), for tests of the cycle; `levels` receives
+ * the hierarchy's depth. */
+dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, const double* r, float* z, int* levels);
+
 /* Benchmark support: the average device time (ms) of each hot kernel of one PCG iteration,
  * launched `reps` times back to back on the handle's stream between CUDA events, on the
  * handle's current data (call after a solve; the solve's output was already returned), and each
