@@ -139,6 +139,26 @@ dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double
  * the hierarchy's depth. */
 dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, const double* r, float* z, int* levels);
 
+/* ---- learned warm start ----------------------------------------------------------------------
+ * No counterpart in the reference: a 4-level U-Net (32/64/128/256 channels, 3 x 3 convolutions,
+ * BF16 weights and activations, FP32 accumulation) that predicts the normalised deflection
+ * w * c / rms(b) from (b / rms(b), (log10(d g) - 22.5) / 1.5). Trained by dt_unet_train_step_dev
+ * (Adam, MSE) on this library's own tensor-core convolution kernels. Shapes: H a multiple of 8,
+ * W a multiple of 512. Device arrays: x [B][H][W][2], targets and predictions [B][H][W] (FP32). */
+typedef struct dt_unet dt_unet;
+dt_status dt_unet_create(int base_channels, unsigned long long seed, dt_unet** out);
+dt_status dt_unet_destroy(dt_unet* u);
+size_t dt_unet_num_params(const dt_unet* u);
+dt_status dt_unet_set_stream(dt_unet* u, void* stream);
+dt_status dt_unet_predict_dev(dt_unet* u, const float* x, float* y, int B, int H, int W);
+dt_status dt_unet_train_step_dev(dt_unet* u, const float* x, const float* t, int B, int H, int W, float lr, double* loss);
+dt_status dt_unet_loss_and_grad_dev(dt_unet* u, const float* x, const float* t, int B, int H, int W, double* loss);
+dt_status dt_unet_gradients(dt_unet* u, float* out, size_t n);
+dt_status dt_unet_get_params(dt_unet* u, float* out, size_t n);
+dt_status dt_unet_set_params(dt_unet* u, const float* in, size_t n);
+dt_status dt_unet_save(dt_unet* u, const char* path);
+dt_status dt_unet_load(dt_unet* u, const char* path);
+
 /* Benchmark support: the average device time (ms) of each hot kernel of one PCG iteration,
  * launched `reps` times back to back on the handle's stream between CUDA events, on the
  * handle's current data (call after a solve; the solve's output was already returned), and each
