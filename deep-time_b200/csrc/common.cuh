@@ -25,6 +25,14 @@ const char* last_error();
     }                                                                                        \
   } while (0)
 
+// DT_CUDA for functions without a status: records the error, which a later DT_CUDA reports.
+#define DT_CUDA_VOID(call)                                                                   \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      ::dt::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_));   \
+  } while (0)
+
 #define DT_TRY(...)               \
   do {                            \
     dt_status s_ = (__VA_ARGS__); \

@@ -865,6 +865,12 @@ struct dt_flex {
   double* scale = nullptr;  // mixed: the residual scale of the current refinement
   dt::WarmInfo* warm = nullptr;
   unsigned char* flush = nullptr;  // benchmark support: an L2-sized scratch buffer, allocated on first use
+  // learned warm start: the model, its cell size, and the coarse input/output buffers
+  dt_unet* unet = nullptr;
+  int unet_f = 0;                  // fine cells per model cell along each axis
+  float *unet_x = nullptr, *unet_y = nullptr;
+  double* unet_sums = nullptr;     // sum of b_coarse^2 and of c
+  double* rzpair = nullptr;        // warm start: b.M^-1 b and r0.M^-1 r0
   std::vector<void*> allocs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
@@ -1224,20 +1230,75 @@ static void norm_b(dt_flex* s, const T* b, Scalars* S) {
   k_take_bb<<<1, 1, 0, s->stream>>>(S); counted();
 }
 
-static dt_status warm_or_cold(dt_flex* s, bool warm) {
+template <class T>
+__global__ void k_add_to64(size_t n, double* __restrict__ x, const T* __restrict__ z) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += (double)z[k];
+}
+
+__global__ void k_keep_rz(const Scalars* S, double* slot) { *slot = S->rz; }
+
+// Keep x0 when its preconditioned residual is below the zero guess's, r0.M^-1 r0 < b.M^-1 b;
+// otherwise x = 0, r = b. The 2-norm of the residual cannot judge a predicted guess: the
+// operator multiplies the prediction's grid-scale rounding noise by up to d lambda^2 / c
+// (1e5 to 1e8 on these rasters), while M^-1 weighs the residual as the error's energy does.
+__global__ void k_warm_decide_pre(size_t n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ b,
+                                  const double* rz) {
+  bool keep = rz[1] < rz[0];
+  if (keep) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] = 0.0;
+    r[k] = b[k];
+  }
+}
+__global__ void k_warm_record_pre(Scalars* S64, const double* rz, WarmInfo* info) {
+  info->accepted = rz[1] < rz[0] ? 1 : 0;
+  info->rel = rz[0] > 0 ? sqrt(rz[1] / rz[0]) : 0.0;
+  if (!info->accepted) S64->rr = S64->bb;
+}
+
+// z = M^-1 v with the lane F (its preconditioner set up), v in FP64; v.z into *slot.
+template <class T>
+static void precond_dot(dt_flex* s, Lane<T>& F, const double* v, int levels, double* slot) {
+  cudaStream_t st = s->stream;
+  k_reset<<<1, 1, 0, st>>>(F.S);
+  counted();
+  const T* vin;
+  if (sizeof(T) == 4) {
+    k_convert<double, T><<<ew_grid(s), 256, 0, st>>>(s->n, v, F.r);
+    counted();
+    vin = F.r;
+  } else {
+    // the FP64 lane preconditions a copy in `ap` (free before the loop), leaving r and b
+    // untouched (the Jacobi sandwich writes `left`, so that cannot hold the input)
+    DT_CUDA_VOID(cudaMemcpyAsync(F.ap, v, s->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    vin = F.ap;
+  }
+  launch_precondition<T>(s, F, vin, F.z, levels, st);
+  k_keep_rz<<<1, 1, 0, st>>>(F.S, slot);
+  counted();
+}
+
+// The first guess: x = 0 (r = b), or the given / predicted guess, kept by the preconditioned
+// residual rule (k_warm_decide_pre).
+template <class T>
+static dt_status warm_or_cold(dt_flex* s, bool warm, Lane<T>& F, int levels) {
   Lane<double>& L = s->L64;
   cudaStream_t st = s->stream;
   if (!warm) {
     k_fill<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, 0.0); counted();
-  }
-  resid64(s);  // r = b - A x (r = b for x = 0)
-  if (warm) {
-    k_warm_decide<double><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, L.S); counted();
-    k_warm_record<<<1, 1, 0, st>>>(L.S, s->warm); counted();
-  } else {
+    resid64(s);  // r = b
     WarmInfo none = {0, 1.0};
     DT_CUDA(cudaMemcpyAsync(s->warm, &none, sizeof none, cudaMemcpyHostToDevice, st));
+    return DT_OK;
   }
+  precond_dot<T>(s, F, s->b64, levels, s->rzpair);  // b . M^-1 b
+  resid64(s);                                       // r0 = b - A x0
+  precond_dot<T>(s, F, L.r, levels, s->rzpair + 1);  // r0 . M^-1 r0
+  k_warm_decide_pre<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, s->rzpair);
+  k_warm_record_pre<<<1, 1, 0, st>>>(L.S, s->rzpair, s->warm);
+  counted();
+  counted();
+  DT_CUDA(cudaGetLastError());
   return DT_OK;
 }
 
@@ -1262,7 +1323,7 @@ static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_r
   DT_TRY(setup_precond<double>(s, L, p->precond, &levels));
   k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
   norm_b<double>(s, s->b64, L.S);
-  DT_TRY(warm_or_cold(s, warm));
+  DT_TRY(warm_or_cold(s, warm, L, levels));
   DT_TRY(run_pcg<double>(s, L, levels, p->host_loop));
   Scalars h;
   DT_TRY(read_scalars(s, L.S, &h));
@@ -1304,7 +1365,7 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
   DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
   k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
   norm_b<double>(s, s->b64, L.S);
-  DT_TRY(warm_or_cold(s, warm));
+  DT_TRY(warm_or_cold(s, warm, F, levels));
   int iterations = 0, refinements = 0;
   Scalars h, hf;
   hf.err = 0.0;
@@ -1452,6 +1513,7 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   if ((st = dalloc(s, &s->partials, cap)) != DT_OK) return fail(st);
   if ((st = dalloc(s, &s->scale, 1)) != DT_OK) return fail(st);
   if ((st = dalloc(s, &s->warm, 1)) != DT_OK) return fail(st);
+  if ((st = dalloc(s, &s->rzpair, 2)) != DT_OK) return fail(st);
   transform_smem_attributes<double>();
   transform_smem_attributes<float>();
   if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
@@ -1481,6 +1543,110 @@ dt_status dt_flex_set_stream(dt_flex* s, void* stream) {
   return DT_OK;
 }
 
+// ---- the learned first guess -------------------------------------------------------------------
+
+// Model inputs at the model's cell size: per coarse cell the block means of b and of
+// log10(d g); sums of b_coarse^2 and of c (for the normalisations) into sums[0..1].
+__global__ void __launch_bounds__(256) k_unet_restrict(int w, int h, int f, const double* __restrict__ d, const double* __restrict__ c,
+                                                       const double* __restrict__ b, float* __restrict__ x, double* partials,
+                                                       unsigned int* ticket, double* sums) {
+  int wc = w / f, hc = h / f;
+  size_t nc = (size_t)wc * hc;
+  double inv = 1.0 / ((double)f * f);
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) {
+    int ic = (int)(k % wc), jc = (int)(k / wc);
+    double sb = 0.0, sl = 0.0, sc = 0.0;
+    for (int dj = 0; dj < f; ++dj)
+      for (int di = 0; di < f; ++di) {
+        size_t q = (size_t)(jc * f + dj) * w + ic * f + di;
+        sb += b[q];
+        sl += log10(d[q] * 9.81);
+        sc += c[q];
+      }
+    double bc = sb * inv;
+    x[2 * k] = (float)bc;
+    x[2 * k + 1] = (float)((sl * inv - 22.5) / 1.5);
+    acc.v[0] += bc * bc;
+    acc.v[1] += sc;
+  }
+  const int kind[2] = {0, 0};
+  if (reduce_partials<2>(acc, kind, partials, ticket, gridDim.x) && threadIdx.x == 0) {
+    sums[0] = acc.v[0];
+    sums[1] = acc.v[1];
+  }
+}
+
+__global__ void k_unet_normalise(size_t nc, float* __restrict__ x, const double* sums) {
+  double rms = sqrt(sums[0] / (double)nc);
+  float inv = rms > 0 ? (float)(1.0 / rms) : 0.f;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) x[2 * k] *= inv;
+}
+
+// The prediction back on the raster, in metres: bilinear from the coarse cells' centres with x
+// wrapping and rows clamping (prolong_linear, flexure.rs:1816-1844), times rms(b_coarse) / mean(c).
+__global__ void k_unet_prolong(int w, int h, int f, const float* __restrict__ y, double* __restrict__ x, const double* sums) {
+  int ws = w / f, hs = h / f;
+  size_t n = (size_t)w * h;
+  double scale = sqrt(sums[0] / ((double)ws * hs)) / (sums[1] / (double)n);
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    int i = (int)(k % w), j = (int)(k / w);
+    double xf = (i + 0.5) / f - 0.5;
+    double yf = fmin(fmax((j + 0.5) / f - 0.5, 0.0), (double)(hs - 1));
+    double x0 = floor(xf), y0 = floor(yf);
+    double tx = xf - x0, ty = yf - y0;
+    int i0 = (((int)x0 % ws) + ws) % ws, i1 = (i0 + 1) % ws;
+    int j0 = (int)y0, j1 = min(j0 + 1, hs - 1);
+    double v = ((double)y[(size_t)j0 * ws + i0] * (1.0 - tx) + (double)y[(size_t)j0 * ws + i1] * tx) * (1.0 - ty) +
+               ((double)y[(size_t)j1 * ws + i0] * (1.0 - tx) + (double)y[(size_t)j1 * ws + i1] * tx) * ty;
+    x[k] = v * scale;
+  }
+}
+
+// x0 of L64 from the model: restrict, normalise, predict on the model's stream, prolong.
+static dt_status unet_first_guess(dt_flex* s) {
+  cudaStream_t st = s->stream;
+  int f = s->unet_f;
+  size_t nc = (size_t)(s->w / f) * (s->h / f);
+  unsigned int g = std::max(1u, std::min<unsigned int>(ceil_div(nc, 256), (unsigned)s->sms * 8));
+  k_unet_restrict<<<g, 256, 0, st>>>(s->w, s->h, f, s->L64.d, s->L64.c, s->b64, s->unet_x, s->partials,
+                                     &s->L64.S->ticket[SITE_MISC], s->unet_sums);
+  k_unet_normalise<<<g, 256, 0, st>>>(nc, s->unet_x, s->unet_sums);
+  counted();
+  counted();
+  DT_CUDA(cudaStreamSynchronize(st));
+  DT_TRY(dt_unet_predict_dev(s->unet, s->unet_x, s->unet_y, 1, s->h / f, s->w / f));
+  k_unet_prolong<<<ew_grid(s), 256, 0, st>>>(s->w, s->h, f, s->unet_y, s->L64.x, s->unet_sums);
+  counted();
+  DT_CUDA(cudaGetLastError());
+  return DT_OK;
+}
+
+dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx) {
+  if (!s) return DT_BAD_ARG;
+  s->unet = nullptr;
+  if (!u) return DT_OK;
+  double ratio = model_dx / s->dx;
+  int f = (int)std::lround(ratio);
+  if (!(model_dx > 0.0) || f < 1 || std::fabs(ratio - f) > 1e-9 * ratio || !is_pow2(f) || s->w % f || s->h % f ||
+      (s->w / f) % 512 || (s->h / f) % 8) {
+    set_error("dt_flex_set_unet: a %d x %d raster of %g m does not coarsen to the model's %g m cells in a shape it takes "
+              "(width a multiple of 512, height of 8, by a power of two)", s->w, s->h, s->dx, model_dx);
+    return DT_UNSUPPORTED;
+  }
+  size_t nc = (size_t)(s->w / f) * (s->h / f);
+  if (!s->unet_x) {
+    DT_TRY(dalloc(s, &s->unet_x, 2 * nc));
+    DT_TRY(dalloc(s, &s->unet_y, nc));
+    DT_TRY(dalloc(s, &s->unet_sums, 2));
+  }
+  s->unet = u;
+  s->unet_f = f;
+  return DT_OK;
+}
+
 static dt_status check_params(const dt_flex_params* p) {
   if (!p) {
     set_error("flexure solve: params is NULL");
@@ -1498,9 +1664,9 @@ static dt_status check_params(const dt_flex_params* p) {
     set_error("flexure solve: unknown precision %d", p->precision);
     return DT_BAD_ARG;
   }
-  if (p->warm_start != DT_WARM_NONE && p->warm_start != DT_WARM_GIVEN) {
-    set_error("flexure solve: warm start %d needs dt_unet (use dt_unet_flex_solve)", p->warm_start);
-    return DT_UNSUPPORTED;
+  if (p->warm_start != DT_WARM_NONE && p->warm_start != DT_WARM_GIVEN && p->warm_start != DT_WARM_UNET) {
+    set_error("flexure solve: unknown warm start %d", p->warm_start);
+    return DT_BAD_ARG;
   }
   return DT_OK;
 }
@@ -1510,6 +1676,13 @@ static dt_status solve_loaded(dt_flex* s, const dt_flex_params* p, dt_report* re
   bool warm = p->warm_start != DT_WARM_NONE;
   long long launches0 = g_launches;
   cudaEventRecord(s->ev0, s->stream);
+  if (p->warm_start == DT_WARM_UNET) {
+    if (!s->unet) {
+      set_error("flexure solve: DT_WARM_UNET without a model (dt_flex_set_unet)");
+      return DT_BAD_ARG;
+    }
+    DT_TRY(unet_first_guess(s));
+  }
   dt_status st = p->precision == DT_PREC_MIXED ? solve_mixed(s, p, warm, rep) : solve_fp64(s, p, warm, rep);
   if (rep) rep->kernel_launches = g_launches - launches0;
   cudaEventRecord(s->ev1, s->stream);

@@ -65,6 +65,7 @@ def lib():
         L.dt_flex_bend.argtypes = [vp, vp, vp, vp]
         L.dt_flex_precondition.argtypes = [vp, vp, vp, vp, vp, i, i]
         L.dt_flex_profile_kernels.argtypes = [vp, i, i, vp, vp]
+        L.dt_flex_set_unet.argtypes = [vp, vp, d]
         _lib = L
     return _lib
 

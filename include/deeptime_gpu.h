@@ -49,7 +49,9 @@ enum { DT_PREC_FP64 = 0,         /* PCG entirely in FP64 */
        DT_PREC_MIXED = 1 };      /* FP32 inner PCG inside FP64 iterative refinement */
 enum { DT_WARM_NONE = 0,         /* start from x = 0 (the reference) */
        DT_WARM_GIVEN = 1,        /* start from x_inout's contents */
-       DT_WARM_UNET = 2 };       /* start from the loaded U-Net's prediction, when it beats x = 0 */
+       DT_WARM_UNET = 2 };       /* start from the attached U-Net's prediction (dt_flex_set_unet);
+                                    a first guess is kept only when its preconditioned residual is
+                                    below the zero guess's (see warm_start_rel_residual) */
 enum { DT_CYCLE_JACOBI = 0,      /* the reference's V-cycle: damped Jacobi, omega 0.8, nu 2, to <= 64 cells */
        DT_CYCLE_RBGS = 1 };      /* red-black Gauss-Seidel V(2,2) to a 16 x 8 coarsest level */
 enum { DT_DIFF_FP64_CG_FP32_CYCLE = 0, /* the reference's split: FP64 CG, FP32 cycle */
@@ -80,7 +82,8 @@ typedef struct {
   double rel_residual;  /* ||b - A x|| / ||b|| at exit (recomputed in FP64) */
   int refinements;      /* MIXED: FP64 refinement steps taken */
   int warm_start_accepted;
-  double warm_start_rel_residual; /* ||b - A x0|| / ||b|| of the offered first guess */
+  double warm_start_rel_residual; /* sqrt(r0.M^-1 r0 / b.M^-1 b) of the offered first guess, r0 = b - A x0,
+                                     M the solve's preconditioner: the guess is kept when it is below 1 */
   double device_ms;     /* device time of the solve (CUDA events on the handle's stream) */
   long long kernel_launches; /* this backend's kernels that ran for the solve */
 } dt_report;
@@ -158,6 +161,11 @@ dt_status dt_unet_get_params(dt_unet* u, float* out, size_t n);
 dt_status dt_unet_set_params(dt_unet* u, const float* in, size_t n);
 dt_status dt_unet_save(dt_unet* u, const char* path);
 dt_status dt_unet_load(dt_unet* u, const char* path);
+/* Attach a model to a flexure handle for DT_WARM_UNET: its first guess is predicted on the model's
+ * cells (model_dx metres, a power-of-two multiple of the raster's dx; block means of b and
+ * log10 D), prolonged bilinearly (prolong_linear, flexure.rs:1816-1844), and kept only when
+ * r0.M^-1 r0 < b.M^-1 b. NULL detaches. */
+dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
 
 /* Benchmark support: the average device time (ms) of each hot kernel of one PCG iteration,
  * launched `reps` times back to back on the handle's stream between CUDA events, on the
