@@ -42,6 +42,8 @@ W, H, DX, SIGMA = 4096, 2048, 2500.0, 32.0
 TOL = 1e-8
 KERNEL_NAMES = ["flex_apply", "cg_update", "cg_direction", "fft_rows_fwd", "dct_cols_divide_idct", "fft_rows_inv_dot",
                 "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_accumulate"]
+WEIGHTS = os.path.join(ROOT, "deep-time_b200", "weights", "unet_flexure.bin")
+MODEL_DX = 10_000.0  # the U-Net's cell size: trained on 512 x 256 rasters of 10 km
 METRIC = "flexure solves/s to relative residual 1e-8 @4096x2048 (time-to-1e-8 per solve = 1000/value ms)"
 
 
@@ -54,6 +56,11 @@ def parse():
     ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
     ap.add_argument("--precond", default="reference", choices=["reference", "mean_d"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the error against the oracle's 1e-12 solve")
+    ap.add_argument("--no-diffusion", action="store_true", help="skip the diffusion solve's leg")
+    ap.add_argument("--warm", default="unet" if os.path.exists(WEIGHTS) else "none", choices=["unet", "none"],
+                    help="first guess of the benchmarked solve (default: the U-Net when trained weights exist)")
+    ap.add_argument("--weights", default=WEIGHTS)
     ap.add_argument("--case", default=None,
                     help="profiling aid (for ncu): run one host-driven, iteration-capped solve and exit; "
                          "'W,H,DX,PRECOND,PRECISION,ITERATIONS' with PRECOND 0 reference / 1 mean-D and PRECISION "
@@ -75,7 +82,9 @@ def run_case(spec):
     print(rep, flush=True)
 
 
-def dist_init(n):
+def dist_init(n, timeout_s=300):
+    """One process per GPU: NCCL when a device is present, gloo otherwise (the host logic's tests).
+    The replicas exchange nothing but the barrier and the max over ranks of the timed region."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -84,8 +93,11 @@ def dist_init(n):
         import torch.distributed as dist
         from datetime import timedelta
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=timeout_s), device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group("gloo", timeout=timedelta(seconds=timeout_s))
     return rank, world, local
 
 
@@ -102,7 +114,8 @@ def max_over_ranks(v, world):
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -249,9 +262,26 @@ def main():
     sv = F.Solver(W, H, DX)
     L.check(lib.dt_flex_set_stream(sv._h, ctypes.c_void_p(stream.cuda_stream)))
     precond = L.PRECOND_REFERENCE if args.precond == "reference" else L.PRECOND_MEAN_D
-    mixed = F.params(precond=precond, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_MIXED, tol=TOL, max_iterations=20000)
-    plain = F.params(precond=L.PRECOND_MEAN_D, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_FP64, tol=TOL,
-                     max_iterations=20000)
+    model = None
+    if args.warm == "unet":
+        if not os.path.exists(args.weights):
+            raise SystemExit(f"--warm unet: no weights at {args.weights} (train them with deep-time_b200/train_unet.py)")
+        from deeptime_gpu import unet as U
+
+        model = U.UNet(seed=1)
+        model.load(args.weights)
+        L.check(lib.dt_flex_set_unet(sv._h, model._h, ctypes.c_double(MODEL_DX)))
+
+    def fp(precision, pc, warm=L.WARM_NONE):
+        return F.params(precond=pc, stop=L.STOP_REL_RESIDUAL, precision=precision, warm_start=warm, tol=TOL,
+                        max_iterations=20000)
+
+    head = fp(L.PREC_MIXED, precond, L.WARM_UNET if model else L.WARM_NONE)
+    methods = {
+        "plain_fp64_gpu": (fp(L.PREC_FP64, L.PRECOND_MEAN_D), "FP64 PCG, constant-mean-D spectral preconditioner"),
+        "fp64_bank_gpu": (fp(L.PREC_FP64, L.PRECOND_REFERENCE), "FP64 PCG, reference 3-level bank + Jacobi"),
+        "mixed_gpu": (fp(L.PREC_MIXED, precond), "mixed precision, zero first guess"),
+    }
 
     def solve_dev(i, p):
         d, c, b = dev[i % len(dev)]
@@ -274,19 +304,27 @@ def main():
         return e0.elapsed_time(e1), reps
 
     for i in range(args.warmup):
-        solve_dev(i, mixed)
+        solve_dev(i, head)
     with Clocks(local) as clk:
-        ms, reps = timed(lambda i: solve_dev(i, mixed), args.steps)
+        ms, reps = timed(lambda i: solve_dev(i, head), args.steps)
     ms = max_over_ranks(ms, world)
     its = [r.iterations for r in reps]
     launches = sum(r.kernel_launches for r in reps)
+    head_ms = ms / args.steps
 
-    # plain FP64 GPU PCG (mean-D preconditioner) on the same inputs: the comparison the target names
-    for i in range(1):
-        solve_dev(i, plain)
-    plain_steps = min(args.steps, 3)
-    pms, preps = timed(lambda i: solve_dev(i, plain), plain_steps)
-    pms = max_over_ranks(pms, world)
+    # the other methods on the same inputs (the comparison the target names is plain_fp64_gpu)
+    breakdown = {}
+    for name, (p, what) in methods.items():
+        solve_dev(0, p)
+        k = min(args.steps, len(dev))
+        pms, preps = timed(lambda i: solve_dev(i, p), k)
+        pms = max_over_ranks(pms, world) / k
+        breakdown[name] = {"ms_per_solve": pms, "iterations": statistics.mean(r.iterations for r in preps),
+                           "method": what, "time_over_value": pms / head_ms}
+    if model:
+        breakdown["warm_start"] = {"accepted": sum(r.warm_start_accepted for r in reps), "of": len(reps),
+                                   "mean_rel_preconditioned_residual": statistics.mean(r.warm_start_rel_residual
+                                                                                       for r in reps)}
 
     # end to end through dt_flex_solve from pinned host buffers
     host = []
@@ -299,7 +337,7 @@ def main():
         d, c, b = host[i % len(host)]
         rep = L.Report()
         st = lib.dt_flex_solve(sv._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(c.data_ptr()),
-                               ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_host.data_ptr()), ctypes.byref(mixed),
+                               ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x_host.data_ptr()), ctypes.byref(head),
                                ctypes.byref(rep))
         L.check(st)
         return rep
@@ -312,7 +350,7 @@ def main():
     # per-kernel launch durations (events) for the roofline
     kms = (ctypes.c_double * 10)()
     kbytes = (ctypes.c_double * 10)()
-    solve_dev(0, mixed)
+    solve_dev(0, methods["mixed_gpu"][0])
     L.check(lib.dt_flex_profile_kernels(sv._h, L.PREC_MIXED, 20, kms, kbytes))
     levels3 = args.precond == "reference"
     per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: 3, 4: 3, 9: 3} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 4: 1, 5: 1})
@@ -327,18 +365,19 @@ def main():
                for k, cnt in per_it.items()}
 
     value = world * args.steps / (ms / 1e3)
+    warm_txt = "U-Net first guess (kept when its preconditioned residual is below the zero guess's)" if model \
+        else "zero first guess"
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic (seeded SplitMix64 fields)",
         "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
                    "method": f"mixed precision (FP32 inner PCG in FP64 refinement), "
-                             f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, zero first guess",
+                             f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, {warm_txt}",
                    "inputs": f"{len(inputs)} seeded input sets cycled, 201 MB each: larger than L2, no flush",
                    "iterations_per_solve": statistics.mean(its), "replicas": world},
-        "plain_fp64_gpu": {"ms_per_solve": pms / plain_steps, "iterations": statistics.mean(r.iterations for r in preps),
-                           "method": "FP64 PCG, constant-mean-D spectral preconditioner",
-                           "speedup_of_value": (pms / plain_steps) / (ms / args.steps)},
+        "plain_fp64_gpu": dict(breakdown["plain_fp64_gpu"], speedup_of_value=breakdown["plain_fp64_gpu"]["ms_per_solve"] / head_ms),
+        "methods": breakdown,
         "e2e": {"value": world * e2e_steps / (ems / 1e3), "unit": "solves/s",
                 "h2d_bytes_per_step": 3 * W * H * 8, "d2h_bytes_per_step": W * H * 8},
         "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[top], "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -347,13 +386,14 @@ def main():
         "clocks": clk.summary(),
         "gpu_launches": launches,
     }
+    if not args.no_diffusion:
+        line["diffusion"] = diffusion_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4))
+    if rank == 0 and not args.no_accuracy:
+        line["accuracy"] = accuracy(lambda p: (solve_dev(0, p), x_dev.cpu().numpy())[1], head, methods, inputs[0])
     if rank == 0 and not args.no_cpu_baseline:
-        from deeptime_gpu import flexure as F2  # noqa: F401
-
         d, c, b = inputs[0]
-        ref_its = solve_dev(0, F.params(precond=L.PRECOND_REFERENCE, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_FP64,
-                                        tol=TOL, max_iterations=20000)).iterations
-        line["cpu_baseline"] = oracle_cpu_baseline(d, c, b, ref_its)
+        ref_its = breakdown["fp64_bank_gpu"]["iterations"]
+        line["cpu_baseline"] = oracle_cpu_baseline(d, c, b, int(round(ref_its)))
     if rank == 0:
         print(json.dumps(line), flush=True)
     sv.close()
@@ -361,6 +401,76 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def diffusion_leg(lib, stream, timed, max_over_ranks, world, steps):
+    """The implicit diffusion solve at 2048 x 1024 (periodic x, closed rows): h a |k|^-2.5 field of
+    std 800 m, kappa dt / dx^2 a smoothed log-uniform field over [0.1, 100] (sigma 8 cells),
+    red-black Gauss-Seidel V(2,2) cycles to 16 x 8, CG to relative residual 1e-10; FP64 against
+    FP32 inner CG + cycle inside FP64 refinement, and the reference's own split (FP64 CG, FP32
+    damped-Jacobi cycle). Device time per solve (inputs resident) and the mixed answer's distance
+    from the FP64 one."""
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import diffusion as D
+    from deeptime_gpu import inputs as I
+
+    w, h, dx, dt = 2048, 1024, 10_000.0, 1.0
+    ws = D.Workspace(D.Dims(w, h, dx, True))
+    L.check(lib.dt_diff_set_stream(ws._h, ctypes.c_void_p(stream.cuda_stream)))
+    sets = [I.diffusion_problem(w, h, 8.0, 3000 + 100 * k) for k in range(2)]
+    dev = [(torch.from_numpy(h0).cuda(), torch.from_numpy(s * dx * dx / dt).cuda()) for h0, s in sets]
+    x = torch.empty_like(dev[0][0])
+
+    def solve(i, p):
+        h0, kd = dev[i % len(dev)]
+        with torch.cuda.stream(stream):
+            x.copy_(h0)
+        rep = L.Report()
+        L.check(lib.dt_diff_solve_dev(ws._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(kd.data_ptr()),
+                                      ctypes.c_double(dt), ctypes.byref(p), ctypes.byref(rep)))
+        return rep
+
+    out = {"workload": f"implicit diffusion {w}x{h}, kappa dt/dx^2 log-uniform [0.1, 100], CG to rel. residual 1e-10"}
+    answers = {}
+    for name, cycle, prec in (("fp64_rbgs", L.CYCLE_RBGS, L.DIFF_FP64), ("mixed_rbgs", L.CYCLE_RBGS, L.DIFF_MIXED),
+                              ("reference_split_jacobi", L.CYCLE_JACOBI, L.DIFF_FP64_CG_FP32_CYCLE)):
+        p = D.params(cycle=cycle, precision=prec, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000)
+        solve(0, p)
+        ms, reps = timed(lambda i: solve(i, p), steps)
+        ms = max_over_ranks(ms, world) / steps
+        solve(0, p)
+        torch.cuda.synchronize()
+        answers[name] = x.clone()
+        out[name] = {"ms_per_solve": ms, "solves_per_s": world * 1e3 / ms,
+                     "iterations": statistics.mean(r.iterations for r in reps),
+                     "rel_residual": max(r.rel_residual for r in reps)}
+    ref = answers["fp64_rbgs"]
+    for name in ("mixed_rbgs", "reference_split_jacobi"):
+        out[name]["rel_l2_vs_fp64"] = float(torch.linalg.norm(answers[name] - ref) / torch.linalg.norm(ref))
+    out["speedup_mixed_vs_fp64"] = out["fp64_rbgs"]["ms_per_solve"] / out["mixed_rbgs"]["ms_per_solve"]
+    ws.close()
+    return out
+
+
+def accuracy(solve_x, head, methods, inp):
+    """Errors of the benchmarked solve (and the plain one) against the oracle's FP64 solve (the
+    reference's preconditioner) to relative residual 1e-12, on the first input set."""
+    from oracle import oracle as O
+
+    d, c, b = inp
+    t = time.perf_counter()
+    xo, rep = O.flex_solve(d, c, b, DX, 1e-12, 5000, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+    secs = time.perf_counter() - t
+    out = {"against": f"oracle FP64 PCG (reference preconditioner) to rel. residual 1e-12 "
+                      f"({rep['iterations']} iterations, {secs:.1f} s on the host), input set 0"}
+    norm = float(np.linalg.norm(xo))
+    for name, p in (("value", head), ("plain_fp64_gpu", methods["plain_fp64_gpu"][0])):
+        x = solve_x(p)
+        out[name] = {"rel_l2": float(np.linalg.norm(x - xo)) / norm, "max_abs_m": float(np.abs(x - xo).max())}
+    out["max_abs_deflection_m"] = float(np.abs(xo).max())
+    return out
 
 
 def read_traffic(kernel):
