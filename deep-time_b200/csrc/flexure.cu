@@ -34,6 +34,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -1896,4 +1897,82 @@ extern "C" dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps
   k_reset<<<1, 1, 0, s->stream>>>(precision == DT_PREC_MIXED ? s->L32.S : s->L64.S);
   cudaStreamSynchronize(s->stream);
   return st;
+}
+
+// =============================================================================================
+// The flexure operator and its energy v.Av with no allocation.
+//
+// For callers that cannot allocate device memory when they need the operator: a host code that
+// has handed the whole device to its own fixed arena, or one that checks a deflection between
+// kernels of its own and must not synchronise the device, as cudaMalloc and cudaFree can. The
+// call needs no solver handle (dt_flex_create allocates the solver's arrays). The reduction's
+// scratch (the solver-state record for the tile kernel, then one partial sum per tile) lives in
+// a file-scope device array of fixed size, found once per device with cudaGetSymbolAddress.
+
+namespace dt {
+
+constexpr size_t NOALLOC_STATE_BYTES = (sizeof(Scalars) + 255) / 256 * 256;
+constexpr size_t NOALLOC_MAX_TILES = DT_NOALLOC_MAX_TILES;
+constexpr size_t NOALLOC_DOUBLES = NOALLOC_STATE_BYTES / sizeof(double) + NOALLOC_MAX_TILES;
+static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+static std::mutex g_noalloc_lock;
+static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// The scratch's device address on the current device: looked up on the first call per device.
+static dt_status noalloc_scratch(double** out) {
+  int dev = -1;
+  DT_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+    set_error("dt_flex_operator_dot_noalloc: device %d beyond the %d this library tracks", dev, NOALLOC_MAX_DEVICES);
+    return DT_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> g(g_noalloc_lock);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    cudaError_t rc = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (rc != cudaSuccess || !p) {
+      set_error("dt_flex_operator_dot_noalloc: cudaGetSymbolAddress on device %d: %s", dev, cudaGetErrorString(rc));
+      return DT_DEVICE_ERROR;
+    }
+    g_noalloc_ptr[dev] = static_cast<double*>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return DT_OK;
+}
+
+}  // namespace dt
+
+extern "C" dt_status dt_flex_operator_dot_noalloc(int w, int h, double dx, const double* d, const double* c, const double* v,
+                                                  double* y, double* vav, void* stream) {
+  if (!d || !c || !v || !y || !vav) {
+    set_error("dt_flex_operator_dot_noalloc: NULL argument");
+    return DT_BAD_ARG;
+  }
+  if (w < 1 || h < 1 || !(dx > 0.0) || !std::isfinite(dx)) {
+    set_error("dt_flex_operator_dot_noalloc: bad raster %d x %d, dx %g", w, h, dx);
+    return DT_BAD_ARG;
+  }
+  const size_t tiles = (size_t)ceil_div((size_t)w, TBX) * ceil_div((size_t)h, tile_rows<double>());
+  if (tiles > NOALLOC_MAX_TILES) {
+    set_error("dt_flex_operator_dot_noalloc: %d x %d needs %zu tiles of %d x %d cells; the fixed scratch holds %zu",
+              w, h, tiles, TBX, tile_rows<double>(), NOALLOC_MAX_TILES);
+    return DT_UNSUPPORTED;
+  }
+  double* scratch = nullptr;
+  DT_TRY(noalloc_scratch(&scratch));
+  Scalars* S = reinterpret_cast<Scalars*>(scratch);
+  double* partials = scratch + NOALLOC_STATE_BYTES / sizeof(double);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // The state record starts at zero every call: no stop flag (the kernel returns at once when one
+  // is set, and a zero v sets one), no graph handle, tickets at zero. Partials need no clearing:
+  // every tile writes its own before the last tile reads them.
+  DT_CUDA(cudaMemsetAsync(S, 0, sizeof(Scalars), st));
+  dim3 grid(ceil_div((size_t)w, TBX), ceil_div((size_t)h, tile_rows<double>())), block(TBX, TTY);
+  k_apply<double, AP_DOT><<<grid, block, 0, st>>>(w, h, 1.0 / (dx * dx), v, nullptr, nullptr, d, c, nullptr, y, partials, S);
+  counted();
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(vav, &S->pap, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  return DT_OK;
 }

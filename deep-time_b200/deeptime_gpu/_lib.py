@@ -66,6 +66,7 @@ def lib():
         L.dt_flex_precondition.argtypes = [vp, vp, vp, vp, vp, i, i]
         L.dt_flex_profile_kernels.argtypes = [vp, i, i, vp, vp]
         L.dt_flex_set_unet.argtypes = [vp, vp, d]
+        L.dt_flex_operator_dot_noalloc.argtypes = [i, i, d, vp, vp, vp, vp, vp, vp]
         _lib = L
     return _lib
 
