@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
     ap.add_argument("--precond", default="reference", choices=["reference", "mean_d"])
+    ap.add_argument("--precision", default="reliable", choices=["reliable", "refinement"],
+                    help="mixed precision of the benchmarked solve: one FP32 PCG with FP64 reliable updates, or FP32 "
+                         "inner PCG inside FP64 iterative refinement (inner tolerance 1e-5)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error against the oracle's 1e-12 solve")
     ap.add_argument("--no-diffusion", action="store_true", help="skip the diffusion solve's leg")
@@ -276,11 +279,13 @@ def main():
         return F.params(precond=pc, stop=L.STOP_REL_RESIDUAL, precision=precision, warm_start=warm, tol=TOL,
                         max_iterations=20000)
 
-    head = fp(L.PREC_MIXED, precond, L.WARM_UNET if model else L.WARM_NONE)
+    head_prec = L.PREC_MIXED_RELIABLE if args.precision == "reliable" else L.PREC_MIXED
+    head = fp(head_prec, precond, L.WARM_UNET if model else L.WARM_NONE)
     methods = {
         "plain_fp64_gpu": (fp(L.PREC_FP64, L.PRECOND_MEAN_D), "FP64 PCG, constant-mean-D spectral preconditioner"),
         "fp64_bank_gpu": (fp(L.PREC_FP64, L.PRECOND_REFERENCE), "FP64 PCG, reference 3-level bank + Jacobi"),
-        "mixed_gpu": (fp(L.PREC_MIXED, precond), "mixed precision, zero first guess"),
+        "mixed_gpu": (fp(L.PREC_MIXED, precond), "FP32 inner PCG in FP64 refinement, zero first guess"),
+        "mixed_reliable_gpu": (fp(L.PREC_MIXED_RELIABLE, precond), "FP32 PCG with FP64 reliable updates, zero first guess"),
     }
 
     def solve_dev(i, p):
@@ -372,7 +377,8 @@ def main():
         "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic (seeded SplitMix64 fields)",
         "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
-                   "method": f"mixed precision (FP32 inner PCG in FP64 refinement), "
+                   "method": ("mixed precision (one FP32 PCG, FP64 reliable updates of x and r), " if args.precision == "reliable"
+                              else "mixed precision (FP32 inner PCG in FP64 refinement), ") +
                              f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, {warm_txt}",
                    "inputs": f"{len(inputs)} seeded input sets cycled, 201 MB each: larger than L2, no flush",
                    "iterations_per_solve": statistics.mean(its), "replicas": world},

@@ -172,6 +172,9 @@ __device__ bool reduce_partials(Acc<NV>& a, const int* kind, double* partials, u
 
 // Kernel launches of the calling thread (eager ones, and those recorded while capturing a graph
 // body); defined in flexure.cu.
+// The U-Net's forward pass on a given stream, without synchronising (defined in unet.cu).
+dt_status unet_predict_on(dt_unet* u, cudaStream_t st, const float* x, float* y, int B, int H, int W);
+
 void count_launch();
 long long launches_now();
 void add_launches(long long k);

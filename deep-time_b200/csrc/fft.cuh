@@ -1,4 +1,4 @@
-// Shared-memory Stockham FFT (radix 8, 4, 2) for power-of-two lengths, written from the
+// Shared-memory Stockham FFT (radix 16, 8, 4, 2) for power-of-two lengths, written from the
 // Stockham autosort formulation as given by Govindaraju et al., "High performance discrete
 // Fourier transforms on graphics processors", SC'08 (their FftIteration): a stage of radix R over
 // sub-transforms of span Ns reads x[j + r N/R], twiddles by e^(-+2 pi i r (j mod Ns)/(Ns R)), takes
@@ -10,18 +10,23 @@
 // threads. Twiddles come from a table tw[t] = e^(-2 pi i t / N) built on the host (long double
 // angles); the inverse transform (unnormalised) conjugates them.
 //
-// Shared-memory layout: element i of a sequence lives at pad(i) = i + (i >> PADSHIFT), one spare
-// slot after every 16 (8-byte complex) or 8 (16-byte complex) values, i.e. every 128 bytes. The
-// stage's strided writes (stride 8 in the first stage) then fall in distinct banks; a sequence
-// occupies padded_len(N) slots.
+// Shared-memory layout: element i of a sequence lives at pad(i) = i + (i >> 4), one spare slot
+// after every 16 values. The first stage's writes (stride 16) then fall in distinct banks for
+// both 8-byte and 16-byte complex values (17 j slots: banks 2j per half warp for float2, 4j per
+// quarter warp for double2); a sequence occupies padded_len(N) slots.
 #pragma once
 #include "common.cuh"
+
+// The largest radix the stages use (16 or 8); a build option for comparing the two.
+#ifndef DT_FFT_MAX_RADIX
+#define DT_FFT_MAX_RADIX 16
+#endif
 
 namespace dt {
 
 template <class C>
 struct Pad {
-  static constexpr int SHIFT = sizeof(C) == 16 ? 3 : 4;
+  static constexpr int SHIFT = 4;
   static __host__ __device__ __forceinline__ constexpr int at(int i) { return i + (i >> SHIFT); }
   static __host__ __device__ __forceinline__ constexpr int len(int n) { return n + (n >> SHIFT) + 1; }
 };
@@ -71,6 +76,46 @@ __device__ __forceinline__ void dft8(C* v) {
   v[7] = csub(e3, t3);
 }
 
+// 16-point DFT as 4 x 4: DFTs of length 4 over the residues mod 4, twiddles W16^(n2 k1), DFTs of
+// length 4 across; X[k1 + 4 k2] lands in v[k1 + 4 k2].
+template <class C, bool INV>
+__device__ __forceinline__ void dft16(C* v) {
+  using T = decltype(C::x);
+  const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173;  // cos, sin of pi/8
+  const T h = (T)0.70710678118654752440;
+  C y[4][4];  // y[n2][k1]
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) {
+    C a0 = v[n2], a1 = v[4 + n2], a2 = v[8 + n2], a3 = v[12 + n2];
+    dft4<C, INV>(a0, a1, a2, a3);
+    y[n2][0] = a0;
+    y[n2][1] = a1;
+    y[n2][2] = a2;
+    y[n2][3] = a3;
+  }
+  // W16^m = e^(-+ i pi m / 8): m = 1, 2, 3 (n2 = 1), 2, 4, 6 (n2 = 2), 3, 6, 9 (n2 = 3)
+  const T sg = INV ? (T)1 : (T)-1;  // sign of the imaginary part of W16^1
+  const C w1 = mk<C>(c1, sg * s1), w2 = mk<C>(h, sg * h), w3 = mk<C>(s1, sg * c1);
+  y[1][1] = cmul(y[1][1], w1);
+  y[1][2] = cmul(y[1][2], w2);
+  y[1][3] = cmul(y[1][3], w3);
+  y[2][1] = cmul(y[2][1], w2);
+  y[2][2] = rot90<C, INV>(y[2][2]);
+  y[2][3] = cmul(y[2][3], mk<C>(-h, sg * h));
+  y[3][1] = cmul(y[3][1], w3);
+  y[3][2] = cmul(y[3][2], mk<C>(-h, sg * h));
+  y[3][3] = cmul(y[3][3], mk<C>(-c1, -sg * s1));
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    C a0 = y[0][k1], a1 = y[1][k1], a2 = y[2][k1], a3 = y[3][k1];
+    dft4<C, INV>(a0, a1, a2, a3);
+    v[k1] = a0;
+    v[k1 + 4] = a1;
+    v[k1 + 8] = a2;
+    v[k1 + 12] = a3;
+  }
+}
+
 // One stage of radix R over the block's sequences of length N = 2^LOGN, each stored at
 // s + b * NP (padded); span NS. Everything but the data is known at compile time, so the index
 // arithmetic is shifts and masks. Threads: batch * N / EPT, each owns EPT / R butterflies.
@@ -80,7 +125,7 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   constexpr int NP = Pad<C>::len(N);
   constexpr int B = EPT / R;
   constexpr int NBF = N / R;
-  constexpr int LOGNBF = LOGN - (R == 8 ? 3 : R == 4 ? 2 : 1);
+  constexpr int LOGNBF = LOGN - (R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1);
   constexpr int STEP = N / (NS * R);
   const int tid = threadIdx.x;
   C v[B][R];
@@ -108,7 +153,9 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < B; ++q) {
-    if (R == 8) {
+    if (R == 16) {
+      dft16<C, INV>(v[q]);
+    } else if (R == 8) {
       dft8<C, INV>(v[q]);
     } else if (R == 4) {
       dft4<C, INV>(v[q][0], v[q][1], v[q][2], v[q][3]);
@@ -121,11 +168,15 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   __syncthreads();
 }
 
-// Stages from span NS on: radix 8 while three or more factors of two remain, then 4 or 2.
+// Stages from span NS on: radix 16 while four or more factors of two remain (and a thread holds
+// 16 values), then 8, 4 or 2.
 template <class C, int EPT, bool INV, int LOGN, int NS, int REM>
 struct Stages {
   static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
-    if constexpr (REM >= 3) {
+    if constexpr (REM >= 4 && EPT % 16 == 0 && DT_FFT_MAX_RADIX >= 16) {
+      stockham_stage<C, 16, EPT, INV, LOGN, NS>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 16, REM - 4>::run(s, tw);
+    } else if constexpr (REM >= 3) {
       stockham_stage<C, 8, EPT, INV, LOGN, NS>(s, tw);
       Stages<C, EPT, INV, LOGN, NS * 8, REM - 3>::run(s, tw);
     } else if constexpr (REM == 2) {

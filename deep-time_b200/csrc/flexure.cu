@@ -71,6 +71,13 @@ struct Scalars {
   double dot_out, max_out;
   unsigned long long cond;  // graph conditional handle, 0 outside a graph
   unsigned int ticket[8];
+  // reliable updates (DT_PREC_MIXED_RELIABLE, FP32 lane only): the sloppy residual is replaced by
+  // the FP64 one, x by the FP64 accumulation, whenever rr has fallen below delta2 * maxrr or
+  // under the tolerance; gate_it == it marks an iteration that does so
+  int reliable;
+  int gate_it;
+  double delta2, maxrr;
+  double rr_true, bb_true;  // ||b - A x||^2 and ||b||^2 in FP64, unscaled
 };
 
 __device__ __forceinline__ void set_cond(Scalars* S, unsigned int v) {
@@ -93,6 +100,18 @@ __device__ void finish_pap(Scalars* S, double pap) {
 __device__ void finish_update(Scalars* S, double rr) {
   S->rr = rr;
   S->it += 1;
+  if (S->reliable) {
+    // the sloppy residual only asks for a replacement; the FP64 residual decides convergence
+    if (!isfinite(rr)) {
+      S->stop = STOP_NONFINITE;
+    } else if (rr <= S->tol * S->tol * S->bb || rr < S->delta2 * S->maxrr) {
+      S->gate_it = S->it;
+    } else if (S->it >= S->max_it) {
+      S->stop = STOP_CAP;
+    }
+    if (S->stop) set_cond(S, 0);
+    return;
+  }
   if (!isfinite(rr)) {
     S->stop = STOP_NONFINITE;
   } else if (S->rule == DT_STOP_REL_RESIDUAL && rr <= S->tol * S->tol * S->bb) {
@@ -179,7 +198,9 @@ enum {
   JAC_LEFT = 2,   // u = J r;         y = r - A u               (preconditioner: left)
   JAC_FINAL = 3,  // u = J r + part;  y = u + J (r - A u), reduce r.y and max|y|
   PLAIN = 4,      // y = A v
-  BEND = 5        // y = L (d L v)
+  BEND = 5,       // y = L (d L v)
+  RESID_GATED = 6 // RESID in an iteration that replaces the residual (S->gate_it == S->it),
+                  // ||y||^2 into S->rr_true; otherwise nothing
 };
 
 // tiles of 64 x 32 cells (FP32) or 64 x 16 (FP64, to stay inside 48 KB of shared memory), 64 x 4
@@ -199,13 +220,21 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
       return;
     }
   }
+  if (MODE == RESID_GATED && S->gate_it != S->it) return;
   constexpr bool JAC = MODE == JAC_LEFT || MODE == JAC_FINAL;
   constexpr int TBY = tile_rows<T>();
   constexpr int SVR = TBY + 4, SVC = TBX + 4, SMR = TBY + 2, SMC = TBX + 2;
+  // c (and b) are staged with the rest, so the output phase reads nothing from global memory;
+  // the FP64 sandwich reads c directly instead (its tiles would pass the 48 KB of static shared
+  // memory)
+  constexpr bool STAGE_C = MODE != BEND && !(JAC && sizeof(T) == 8);
+  constexpr bool STAGE_B = MODE == RESID || MODE == RESID_GATED;
   __shared__ T sv[SVR][SVC];                        // the vector, 2-cell halo (JAC: r)
   __shared__ T sJ[JAC ? SVR : 1][JAC ? SVC : 1];    // JAC: J
-  __shared__ T sP[MODE == JAC_FINAL ? SVR : 1][MODE == JAC_FINAL ? SVC : 1];  // JAC_FINAL: part
+  __shared__ T sP[JAC ? SVR : 1][JAC ? SVC : 1];    // JAC_FINAL: part; then (JAC) u
   __shared__ T sd[SMR][SMC];                        // d, 1-cell halo; then m = d L v in place
+  __shared__ T sc[STAGE_C ? TBY : 1][STAGE_C ? TBX : 1];  // c on the tile
+  __shared__ T sB[STAGE_B ? TBY : 1][STAGE_B ? TBX : 1];  // b on the tile
   const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + ty * TBX;
@@ -238,20 +267,31 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
     __pipeline_memcpy_async(&sd[mj][tx], d + row + ma, sizeof(T));
     if (extra_m) __pipeline_memcpy_async(&sd[mj][TBX + tx], d + row + mb, sizeof(T));
   }
+  if (STAGE_C || STAGE_B) {
+    const int ic = i0 + tx;
+    for (int oj = ty; oj < TBY; oj += TTY) {
+      int jc = j0 + oj;
+      if (ic < w && jc < h) {
+        size_t k = (size_t)jc * w + ic;
+        if (STAGE_C) __pipeline_memcpy_async(&sc[oj][tx], c + k, sizeof(T));
+        if (STAGE_B) __pipeline_memcpy_async(&sB[oj][tx], rb + k, sizeof(T));
+      }
+    }
+  }
   __pipeline_commit();
   __pipeline_wait_prior(0);
   __syncthreads();
   if (JAC) {
-    // the vector the mode forms: u = J r (+ part); r stays readable for the outputs
+    // the vector the mode forms: u = J r (+ part); r and J stay readable for the outputs
     for (int idx = tid; idx < SVR * SVC; idx += TBX * TTY) {
       int jj = idx / SVC, ii = idx - jj * SVC;
       T u = sJ[jj][ii] * sv[jj][ii];
       if (MODE == JAC_FINAL) u += sP[jj][ii];
-      sJ[jj][ii] = u;  // sJ now holds u
+      sP[jj][ii] = u;  // sP now holds u
     }
     __syncthreads();
   }
-  T(*su)[SVC] = JAC ? reinterpret_cast<T(*)[SVC]>(&sJ[0][0]) : sv;
+  T(*su)[SVC] = JAC ? reinterpret_cast<T(*)[SVC]>(&sP[0][0]) : sv;
   // m = d . L u on the tile plus a 1-cell halo (rows of m clamp the same way)
   for (int mj = ty; mj < SMR; mj += TTY) {
     int gm = min(max(j0 - 1 + mj, 0), h - 1);
@@ -286,21 +326,21 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
       if (MODE == BEND) {
         y[k] = lm;
       } else {
-        T au = lm + c[k] * u;
+        T au = lm + (STAGE_C ? sc[oj][oi] : c[k]) * u;
         if (MODE == AP_DOT) {
           y[k] = au;
           acc.v[0] += (double)u * (double)au;
         } else if (MODE == PLAIN) {
           y[k] = au;
-        } else if (MODE == RESID) {
-          T rr = rb[k] - au;
+        } else if (MODE == RESID || MODE == RESID_GATED) {
+          T rr = (STAGE_B ? sB[oj][oi] : rb[k]) - au;
           y[k] = rr;
           acc.v[0] += (double)rr * (double)rr;
         } else if (MODE == JAC_LEFT) {
           y[k] = sv[oj + 2][oi + 2] - au;
         } else {  // JAC_FINAL
           T r = sv[oj + 2][oi + 2];
-          T z = u + J[k] * (r - au);
+          T z = u + sJ[oj + 2][oi + 2] * (r - au);
           y[k] = z;
           acc.v[0] += (double)r * (double)z;
           acc.v[1] = fmax(acc.v[1], fabs((double)z));
@@ -308,15 +348,16 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
       }
     }
   }
-  if (MODE == AP_DOT || MODE == RESID || MODE == JAC_FINAL) {
+  if (MODE == AP_DOT || MODE == RESID || MODE == RESID_GATED || MODE == JAC_FINAL) {
     const int kind[2] = {0, 1};
     unsigned int nb = gridDim.x * gridDim.y;
-    int site = MODE == AP_DOT ? SITE_PAP : MODE == RESID ? SITE_RESID : SITE_PRECOND;
+    int site = MODE == AP_DOT ? SITE_PAP : (MODE == RESID || MODE == RESID_GATED) ? SITE_RESID : SITE_PRECOND;
     bool last = MODE == JAC_FINAL ? reduce_partials<2>(acc, kind, partials, &S->ticket[site], nb)
                                   : reduce_partials<1>(*reinterpret_cast<Acc<1>*>(&acc), kind, partials, &S->ticket[site], nb);
     if (last && tid == 0) {
       if (MODE == AP_DOT) finish_pap(S, acc.v[0]);
       if (MODE == RESID) S->rr = acc.v[0];
+      if (MODE == RESID_GATED) S->rr_true = acc.v[0];
       if (MODE == JAC_FINAL) finish_precond(S, acc.v[0], acc.v[1]);
     }
   }
@@ -382,6 +423,60 @@ __global__ void k_scale_down(size_t n, const double* __restrict__ r, float* __re
 __global__ void k_accumulate(size_t n, double* __restrict__ x, const float* __restrict__ e32, const double* scale) {
   double inv = 1.0 / *scale;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += (double)e32[k] * inv;
+}
+
+// Reliable updates (the sloppy lane holds r32 = s r64 and its correction x32 = s e). In an
+// iteration that replaces the residual (gate_it == it):
+//   k_reliable_accumulate  x64 += x32 / s; x32 = 0
+//   k_apply<double, RESID_GATED>  r64 = b - A x64, ||r64||^2 -> rr_true
+//   k_reliable_reset       r32 = s r64; rr, maxrr from rr_true; stop when rr_true meets the
+//                          tolerance
+__global__ void k_reliable_accumulate(size_t n, double* __restrict__ x, float* __restrict__ e32, const double* scale,
+                                      const Scalars* S) {
+  if (S->stop || S->gate_it != S->it) return;
+  double inv = 1.0 / *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] += (double)e32[k] * inv;
+    e32[k] = 0.0f;
+  }
+}
+
+__global__ void k_reliable_reset(size_t n, const double* __restrict__ r, float* __restrict__ r32, const double* scale,
+                                 Scalars* S) {
+  if (S->stop || S->gate_it != S->it) return;
+  double sc = *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    r32[k] = (float)(r[k] * sc);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double rr = S->rr_true * sc * sc;
+    S->rr = rr;
+    S->maxrr = rr;
+    if (!isfinite(S->rr_true)) {
+      S->stop = STOP_NONFINITE;
+    } else if (S->rr_true <= S->tol * S->tol * S->bb_true) {
+      S->stop = STOP_CONVERGED;
+    }
+    if (S->stop) set_cond(S, 0);
+  }
+}
+
+// The FP32 lane's problem for reliable updates, from the FP64 lane's (bb, rr of r = b - A x) and
+// the scale s of r32 = s r. The tolerance is on the relative residual, or with `rms` on the RMS
+// residual (||r||^2 <= tol^2 n).
+__global__ void k_reliable_init(Scalars* F, const Scalars* S64, const double* scale, double tol, int max_it, double delta,
+                                int rms) {
+  double s2 = (*scale) * (*scale);
+  double bref = rms ? (double)S64->n : S64->bb;
+  F->tol = tol;
+  F->max_it = max_it;
+  F->rule = DT_STOP_REL_RESIDUAL;
+  F->bb = bref * s2;
+  F->bb_true = bref;
+  F->rr = S64->rr * s2;
+  F->maxrr = F->rr;
+  F->delta2 = delta * delta;
+  F->gate_it = -1;
+  F->reliable = 1;
 }
 
 template <class T>
@@ -477,7 +572,7 @@ __host__ __device__ constexpr int rows_per_block(int logn) { return (32 * FFT_EP
 // 100 KB of padded shared memory, 8 columns.
 __host__ __device__ constexpr int cols_per_block(int logh, int elem) {
   int h = 1 << logh;
-  int plen = elem == 16 ? h + (h >> 3) + 1 : h + (h >> 4) + 1;
+  int plen = h + (h >> 4) + 1;
   int cpb = (32 * FFT_EPT >> logh) > 1 ? (32 * FFT_EPT >> logh) : 1;
   while (cpb < 8 && cpb * 2 * h <= FFT_MAX_THREADS * FFT_EPT && cpb * 2 * plen * elem <= 102400) cpb *= 2;
   return cpb;
@@ -844,9 +939,9 @@ struct Lane {
   cplx<T>* half = nullptr;
   Tables<T> tab;
   Scalars* S = nullptr;
-  cudaGraph_t graph[2] = {nullptr, nullptr};  // [levels == 3]
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  long long body_kernels[2] = {0, 0};         // kernels in one pass of each loop body
+  cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
+  cudaGraphExec_t exec[4] = {};
+  long long body_kernels[4] = {};  // kernels in one pass of each loop body
 };
 
 static const long double PI_L = 3.14159265358979323846264338327950288L;
@@ -941,7 +1036,7 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
 
 template <class T>
 static void free_graphs(Lane<T>& L) {
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 4; ++k) {
     if (L.exec[k]) cudaGraphExecDestroy(L.exec[k]);
     if (L.graph[k]) cudaGraphDestroy(L.graph[k]);
     L.exec[k] = nullptr;
@@ -963,6 +1058,7 @@ static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* 
     case JAC_FINAL: k_apply<T, JAC_FINAL><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
     case PLAIN: k_apply<T, PLAIN><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
     case BEND: k_apply<T, BEND><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
+    case RESID_GATED: k_apply<T, RESID_GATED><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
   }
 }
 
@@ -1086,19 +1182,34 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
   launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, r, z, L.S, st);  // z = u + J(r - A u)
 }
 
-// One PCG iteration (flexure.rs:1709-1738): the body of the device loop.
+// The residual replacement of a reliable-update iteration (FP32 lane): gated kernels that do
+// nothing unless the iteration's update asked for it.
+static void launch_reliable(dt_flex* s, cudaStream_t st) {
+  Lane<double>& L = s->L64;
+  Lane<float>& F = s->L32;
+  k_reliable_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale, F.S); counted();
+  launch_apply<double>(s, RESID_GATED, L.x, nullptr, nullptr, L.d, L.c, s->b64, L.r, F.S, st);
+  k_reliable_reset<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, s->scale, F.S); counted();
+}
+
+// One PCG iteration (flexure.rs:1709-1738): the body of the device loop. With `reliable` (FP32
+// lane) the residual replacement sits between the update and the preconditioner, so z, beta and
+// p follow the replaced residual and the search direction carries on.
 template <class T>
-static void launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st) {
+static void launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st, bool reliable = false) {
   launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st);
   k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); counted();
+  if constexpr (sizeof(T) == 4) {
+    if (reliable) launch_reliable(s, st);
+  }
   launch_precondition<T>(s, L, L.r, L.z, levels, st);
   k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); counted();
 }
 
 // The loop graph: k_arm -> WHILE(iteration) -> k_disarm. Built once per lane and level count.
 template <class T>
-static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* out) {
-  int li = levels == 3 ? 1 : 0;
+static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* out, bool reliable = false) {
+  int li = (levels == 3 ? 1 : 0) + (reliable ? 2 : 0);
   if (L.exec[li]) {
     *out = L.exec[li];
     return DT_OK;
@@ -1127,7 +1238,7 @@ static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* 
   DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   g_capturing = true;
   g_captured = 0;
-  launch_iteration<T>(s, L, levels, s->stream);
+  launch_iteration<T>(s, L, levels, s->stream, reliable);
   g_capturing = false;
   L.body_kernels[li] = g_captured;
   cudaGraph_t captured;
@@ -1173,6 +1284,8 @@ __global__ void k_put_problem(Scalars* S, HostProblem p) {
   S->max_it = p.max_it;
   S->rule = p.rule;
   S->n = p.n;
+  S->reliable = 0;
+  S->gate_it = -1;
 }
 
 // PCG of lane L from its x (guess), r = b - A x and S->rr, S->bb already set: the first
@@ -1186,7 +1299,7 @@ static dt_status read_scalars(dt_flex* s, const Scalars* S, Scalars* out) {
 // host_loop: 0 the device-side graph loop; 1 a host loop with one sync per iteration; 2 the same
 // with each iteration's scalars printed to stderr. Returns with the solve enqueued (graph) or done.
 template <class T>
-static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop) {
+static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop, bool reliable = false) {
   cudaStream_t st = s->stream;
   k_begin<<<1, 1, 0, st>>>(L.S); counted();
   launch_precondition<T>(s, L, L.r, L.z, levels, st);
@@ -1194,28 +1307,29 @@ static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop) {
   DT_CUDA(cudaMemcpyAsync(L.p, L.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
   if (!host_loop) {
     cudaGraphExec_t exec;
-    DT_TRY(loop_exec<T>(s, L, levels, &exec));
+    DT_TRY(loop_exec<T>(s, L, levels, &exec, reliable));
     DT_CUDA(cudaGraphLaunch(exec, st));
     return DT_OK;
   }
   Scalars h;
   DT_TRY(read_scalars(s, L.S, &h));
   for (int pass = 0; pass < h.max_it + 2 && h.stop == STOP_RUNNING; ++pass) {
-    launch_iteration<T>(s, L, levels, st);
+    launch_iteration<T>(s, L, levels, st, reliable);
     DT_CUDA(cudaGetLastError());
     DT_TRY(read_scalars(s, L.S, &h));
     if (host_loop > 1)
-      fprintf(stderr, "pcg(%s) it %d stop %d rr %.6e rz %.6e pap %.6e alpha %.6e beta %.6e err %.6e\n",
-              sizeof(T) == 8 ? "fp64" : "fp32", h.it, h.stop, h.rr, h.rz, h.pap, h.alpha, h.beta, h.err);
+      fprintf(stderr, "pcg(%s) it %d stop %d rr %.6e rz %.6e pap %.6e alpha %.6e beta %.6e err %.6e%s\n",
+              sizeof(T) == 8 ? "fp64" : "fp32", h.it, h.stop, h.rr, h.rz, h.pap, h.alpha, h.beta, h.err,
+              h.reliable && h.gate_it == h.it ? " (residual replaced)" : "");
   }
   return DT_OK;
 }
 
 // Kernels the graph loop ran in its last launch (arm and disarm, and a body per pass).
 template <class T>
-static void count_loop(const Lane<T>& L, int levels, int host_loop, int body_runs) {
+static void count_loop(const Lane<T>& L, int levels, int host_loop, int body_runs, bool reliable = false) {
   if (host_loop) return;
-  g_launches += 2 + L.body_kernels[levels == 3 ? 1 : 0] * (long long)body_runs;
+  g_launches += 2 + L.body_kernels[(levels == 3 ? 1 : 0) + (reliable ? 2 : 0)] * (long long)body_runs;
 }
 
 // r = b - A x in FP64 with ||r||^2 into S->rr.
@@ -1405,6 +1519,58 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
   DT_TRY(read_scalars(s, L.S, &h));
   h.err = hf.err;
   DT_TRY(fill_report(s, h, iterations, refinements, rep));
+  if (rep) {
+    rep->converged = converged;
+    rep->rel_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
+  }
+  if (nonfinite) {
+    set_error("flexure solve: a non-finite value appeared");
+    return DT_NONFINITE;
+  }
+  return converged ? DT_OK : DT_NOT_CONVERGED;
+}
+
+// FP32 PCG with reliable updates (the mixed-precision CG of lattice QCD solvers: Clark et al.,
+// "Solving lattice QCD systems of equations using mixed precision solvers on GPUs", 2010). One
+// FP32 Krylov sequence runs to the end; whenever its residual has fallen by RELIABLE_DELTA since
+// the last replacement (or under the tolerance), the correction is added to the FP64 solution,
+// the FP64 residual b - A x replaces the FP32 one and the search direction carries on. The FP64
+// residual alone decides convergence. Unlike refinement, no restart throws the Krylov space away.
+constexpr double RELIABLE_DELTA = 0.1;
+
+static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool warm, dt_report* rep) {
+  Lane<double>& L = s->L64;
+  Lane<float>& F = s->L32;
+  cudaStream_t st = s->stream;
+  if (p->stop == DT_STOP_MAX_Z) {
+    set_error("flexure solve: the mixed-precision path stops on a residual rule (DT_STOP_REL_RESIDUAL or DT_STOP_RMS_RESIDUAL)");
+    return DT_UNSUPPORTED;
+  }
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d); counted();
+  k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
+  int levels = 1;
+  DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
+  norm_b<double>(s, s->b64, L.S);
+  DT_TRY(warm_or_cold(s, warm, F, levels));
+  k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale); counted();
+  k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{p->tol, p->max_iterations, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
+  k_reliable_init<<<1, 1, 0, st>>>(F.S, L.S, s->scale, p->tol, p->max_iterations, RELIABLE_DELTA,
+                                   p->stop == DT_STOP_RMS_RESIDUAL ? 1 : 0);
+  counted();
+  DT_TRY(run_pcg<float>(s, F, levels, p->host_loop, true));
+  // the correction the FP32 lane holds since its last replacement, and the true residual
+  k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale); counted();
+  resid64(s);
+  Scalars h, hf;
+  DT_TRY(read_scalars(s, F.S, &hf));
+  count_loop(F, levels, p->host_loop, hf.body_runs, true);
+  DT_TRY(read_scalars(s, L.S, &h));
+  bool nonfinite = hf.stop == STOP_NONFINITE || !std::isfinite(h.rr) || !std::isfinite(h.bb);
+  double bref = p->stop == DT_STOP_RMS_RESIDUAL ? (double)s->n : h.bb;
+  bool converged = !nonfinite && (h.bb <= 0 || h.rr <= p->tol * p->tol * bref);
+  h.err = hf.err;
+  DT_TRY(fill_report(s, h, hf.it, 0, rep));
   if (rep) {
     rep->converged = converged;
     rep->rel_residual = h.bb > 0 ? std::sqrt(h.rr / h.bb) : 0.0;
@@ -1617,8 +1783,8 @@ static dt_status unet_first_guess(dt_flex* s) {
   k_unet_normalise<<<g, 256, 0, st>>>(nc, s->unet_x, s->unet_sums);
   counted();
   counted();
-  DT_CUDA(cudaStreamSynchronize(st));
-  DT_TRY(dt_unet_predict_dev(s->unet, s->unet_x, s->unet_y, 1, s->h / f, s->w / f));
+  // the model runs on the solve's stream, in order with the kernels around it
+  DT_TRY(unet_predict_on(s->unet, st, s->unet_x, s->unet_y, 1, s->h / f, s->w / f));
   k_unet_prolong<<<ew_grid(s), 256, 0, st>>>(s->w, s->h, f, s->unet_y, s->L64.x, s->unet_sums);
   counted();
   DT_CUDA(cudaGetLastError());
@@ -1661,7 +1827,7 @@ static dt_status check_params(const dt_flex_params* p) {
     set_error("flexure solve: bad stopping rule (rule %d, tol %g, max_iterations %d)", p->stop, p->tol, p->max_iterations);
     return DT_BAD_ARG;
   }
-  if (p->precision != DT_PREC_FP64 && p->precision != DT_PREC_MIXED) {
+  if (p->precision != DT_PREC_FP64 && p->precision != DT_PREC_MIXED && p->precision != DT_PREC_MIXED_RELIABLE) {
     set_error("flexure solve: unknown precision %d", p->precision);
     return DT_BAD_ARG;
   }
@@ -1684,7 +1850,9 @@ static dt_status solve_loaded(dt_flex* s, const dt_flex_params* p, dt_report* re
     }
     DT_TRY(unet_first_guess(s));
   }
-  dt_status st = p->precision == DT_PREC_MIXED ? solve_mixed(s, p, warm, rep) : solve_fp64(s, p, warm, rep);
+  dt_status st = p->precision == DT_PREC_MIXED            ? solve_mixed(s, p, warm, rep)
+                 : p->precision == DT_PREC_MIXED_RELIABLE ? solve_mixed_reliable(s, p, warm, rep)
+                                                          : solve_fp64(s, p, warm, rep);
   if (rep) rep->kernel_launches = g_launches - launches0;
   cudaEventRecord(s->ev1, s->stream);
   cudaError_t e = cudaEventSynchronize(s->ev1);

@@ -244,6 +244,7 @@ struct dt_unet {
   double* loss_part = nullptr;
   std::vector<void*> batch_allocs, allocs;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;  // false once bound to a caller's stream (dt_unet_set_stream)
   int sms = 148;
 };
 
@@ -565,6 +566,20 @@ static dt_status unet_check_shape(int B, int H, int W) {
   return DT_OK;
 }
 
+// The forward pass on stream `st`, in stream order (no synchronisation): for callers that run the
+// model between kernels of their own (the flexure solve's first guess).
+dt_status unet_predict_on(dt_unet* u, cudaStream_t st, const float* x, float* y, int B, int H, int W) {
+  if (!u || !x || !y) return DT_BAD_ARG;
+  DT_TRY(unet_check_shape(B, H, W));
+  DT_TRY(unet_batch(u, B, H, W));
+  size_t npix = (size_t)B * H * W;
+  k_pack_input<<<ugrid(u, npix), 256, 0, st>>>(npix, x, u->X0);
+  count_launch();
+  unet_forward(u, st);
+  DT_CUDA(cudaMemcpyAsync(y, u->pred, npix * sizeof(float), cudaMemcpyDeviceToDevice, st));
+  return DT_OK;
+}
+
 }  // namespace dt
 
 using namespace dt;
@@ -599,7 +614,7 @@ dt_status dt_unet_destroy(dt_unet* u) {
   if (u->stream) cudaStreamSynchronize(u->stream);
   for (void* p : u->batch_allocs) cudaFree(p);
   for (void* p : u->allocs) cudaFree(p);
-  if (u->stream) cudaStreamDestroy(u->stream);
+  if (u->stream && u->own_stream) cudaStreamDestroy(u->stream);
   delete u;
   return DT_OK;
 }
@@ -608,26 +623,22 @@ size_t dt_unet_num_params(const dt_unet* u) { return u ? u->n_params : 0; }
 
 dt_status dt_unet_set_stream(dt_unet* u, void* stream) {
   if (!u) return DT_BAD_ARG;
+  if (stream && (cudaStream_t)stream == u->stream) return DT_OK;
   cudaStreamSynchronize(u->stream);
-  cudaStreamDestroy(u->stream);
+  if (u->own_stream) cudaStreamDestroy(u->stream);
   if (stream) {
     u->stream = (cudaStream_t)stream;
-  } else if (cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    return DT_DEVICE_ERROR;
+    u->own_stream = false;
+  } else {
+    if (cudaStreamCreateWithFlags(&u->stream, cudaStreamNonBlocking) != cudaSuccess) return DT_DEVICE_ERROR;
+    u->own_stream = true;
   }
   return DT_OK;
 }
 
 // x: [B][H][W][2] FP32 (device), y: [B][H][W] FP32 (device)
 dt_status dt_unet_predict_dev(dt_unet* u, const float* x, float* y, int B, int H, int W) {
-  if (!u || !x || !y) return DT_BAD_ARG;
-  DT_TRY(unet_check_shape(B, H, W));
-  DT_TRY(unet_batch(u, B, H, W));
-  size_t npix = (size_t)B * H * W;
-  k_pack_input<<<ugrid(u, npix), 256, 0, u->stream>>>(npix, x, u->X0);
-  count_launch();
-  unet_forward(u, u->stream);
-  DT_CUDA(cudaMemcpyAsync(y, u->pred, npix * sizeof(float), cudaMemcpyDeviceToDevice, u->stream));
+  DT_TRY(dt::unet_predict_on(u, u ? u->stream : nullptr, x, y, B, H, W));
   DT_CUDA(cudaStreamSynchronize(u->stream));
   return DT_OK;
 }

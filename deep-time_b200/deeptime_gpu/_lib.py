@@ -13,7 +13,7 @@ STATUS_NAMES = {0: "DT_OK", 1: "DT_NOT_CONVERGED", 2: "DT_NONFINITE", 3: "DT_OOM
                 6: "DT_UNSUPPORTED"}
 PRECOND_REFERENCE, PRECOND_MEAN_D = 0, 1
 STOP_MAX_Z, STOP_REL_RESIDUAL, STOP_RMS_RESIDUAL = 0, 1, 2
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_RELIABLE = 0, 1, 2
 WARM_NONE, WARM_GIVEN, WARM_UNET = 0, 1, 2
 CYCLE_JACOBI, CYCLE_RBGS = 0, 1
 DIFF_FP64_CG_FP32_CYCLE, DIFF_FP64, DIFF_MIXED = 0, 1, 2

@@ -46,7 +46,10 @@ enum { DT_STOP_MAX_Z = 0,        /* the reference's: max |z| < tol metres (flexu
        DT_STOP_REL_RESIDUAL = 1, /* ||b - A x||_2 / ||b||_2 <= tol */
        DT_STOP_RMS_RESIDUAL = 2 };/* the reference diffusion's: ||r||_2^2 <= tol^2 n (multigrid.rs:620) */
 enum { DT_PREC_FP64 = 0,         /* PCG entirely in FP64 */
-       DT_PREC_MIXED = 1 };      /* FP32 inner PCG inside FP64 iterative refinement */
+       DT_PREC_MIXED = 1,        /* FP32 inner PCG inside FP64 iterative refinement */
+       DT_PREC_MIXED_RELIABLE = 2 }; /* one FP32 PCG whose residual is replaced by the FP64 b - A x
+                                        (and its correction added to the FP64 x) each time it has
+                                        fallen tenfold; the FP64 residual decides convergence */
 enum { DT_WARM_NONE = 0,         /* start from x = 0 (the reference) */
        DT_WARM_GIVEN = 1,        /* start from x_inout's contents */
        DT_WARM_UNET = 2 };       /* start from the attached U-Net's prediction (dt_flex_set_unet);

@@ -170,18 +170,37 @@ def test_baseline_plain_fp64_matches_the_oracle(precond):
     assert rel_l2(x, xo) < 1e-8
 
 
+@pytest.mark.parametrize("precision", [L.PREC_MIXED, L.PREC_MIXED_RELIABLE])
 @pytest.mark.parametrize("precond", [L.PRECOND_MEAN_D, L.PRECOND_REFERENCE])
-def test_mixed_precision_reaches_the_fp64_answer(precond):
-    # FP32 inner PCG inside FP64 refinement to 1e-8, at the fine-grid conditioning (dx 2.5 km)
+def test_mixed_precision_reaches_the_fp64_answer(precond, precision):
+    # FP32 PCG inside FP64 refinement, or with FP64 reliable updates, to 1e-8 at the fine-grid
+    # conditioning (dx 2.5 km)
     w, h, dx = 512, 256, 2500.0
     d, c, b = I.flexure_problem(w, h, 32.0, 1200)
     xo, ro = O.flex_solve(d, c, b, dx, 1e-12, 10000, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
     sv = F.Solver(w, h, dx)
-    p = F.params(precond=precond, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_MIXED, tol=1e-8, max_iterations=20000)
+    p = F.params(precond=precond, stop=L.STOP_REL_RESIDUAL, precision=precision, tol=1e-8, max_iterations=20000)
     x, rep = sv.solve_with(d, c, b, p)
     assert rep.converged, rep
     assert rep.rel_residual <= 1e-8
     assert rel_l2(x, xo) < 1e-8
+
+
+def test_reliable_updates_take_about_the_fp64_iterations():
+    # one FP32 Krylov sequence with FP64 residual replacements: no restarts, so the iteration count
+    # stays near the FP64 solve's (refinement restarts and needs more)
+    w, h, dx = 512, 256, 2500.0
+    d, c, b = I.flexure_problem(w, h, 32.0, 1201)
+    sv = F.Solver(w, h, dx)
+    its = {}
+    for precision in (L.PREC_FP64, L.PREC_MIXED_RELIABLE):
+        p = F.params(precond=L.PRECOND_REFERENCE, stop=L.STOP_REL_RESIDUAL, precision=precision, tol=1e-8,
+                     max_iterations=20000)
+        x, rep = sv.solve_with(d, c, b, p)
+        assert rep.converged and rep.rel_residual <= 1e-8
+        its[precision] = rep.iterations
+    print(its)
+    assert its[L.PREC_MIXED_RELIABLE] <= 1.25 * its[L.PREC_FP64] + 2, its
 
 
 def test_a_given_first_guess_is_kept_only_when_it_beats_zero():
