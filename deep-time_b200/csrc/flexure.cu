@@ -564,6 +564,7 @@ enum { INV_STORE = 0, INV_ACCUM = 1, INV_STORE_DOT = 2, INV_STORE_W = 3 };
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
 constexpr int FFT_EPT = 16;
+constexpr int FFT_BATCH = 8;  // global loads a thread of a transform kernel keeps in flight
 constexpr int FFT_MAX_THREADS = 512;
 
 // Rows per block so that a block has at least one warp.
@@ -592,28 +593,42 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   constexpr int RB = rows_per_block(LOGN);
   const int row0 = blockIdx.x * RB;
   const int tid = threadIdx.x;
-  // load rows as complex pairs (v[2n], v[2n+1]): one 2-wide vector load per pair
+  // load rows as complex pairs (v[2n], v[2n+1]): one 2-wide vector load per pair. The block has
+  // NT threads (fft_geometry), FFT_EPT pairs each; loads go out in batches before the shared
+  // stores so that a thread keeps FFT_BATCH of them in flight.
+  constexpr int NT = RB * N / FFT_EPT;
+  static_assert(NT * FFT_EPT == RB * N, "rows: whole pairs per thread");
 #pragma unroll 1
-  for (int idx = tid; idx < RB * N; idx += blockDim.x) {
-    int rb = idx >> logN, nn = idx & (N - 1);
-    int j = row0 + rb;
-    C z = mk<C>((T)0, (T)0);
-    if (j < h) {
-      size_t k = (size_t)j * w + 2 * nn;
-      z = *reinterpret_cast<const C*>(v + k);
-      if (WEIGHT) {
-        C ww = *reinterpret_cast<const C*>(wt + k);
-        z.x *= ww.x;
-        z.y *= ww.y;
+  for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
+    C zb[FFT_BATCH];
+#pragma unroll
+    for (int u = 0; u < FFT_BATCH; ++u) {
+      int idx = tid + (q0 + u) * NT;
+      int rb = idx >> logN, nn = idx & (N - 1);
+      int j = row0 + rb;
+      C z = mk<C>((T)0, (T)0);
+      if (j < h) {
+        size_t k = (size_t)j * w + 2 * nn;
+        z = *reinterpret_cast<const C*>(v + k);
+        if (WEIGHT) {
+          C ww = *reinterpret_cast<const C*>(wt + k);
+          z.x *= ww.x;
+          z.y *= ww.y;
+        }
       }
+      zb[u] = z;
     }
-    s[rb * NP + P::at(nn)] = z;
+#pragma unroll
+    for (int u = 0; u < FFT_BATCH; ++u) {
+      int idx = tid + (q0 + u) * NT;
+      s[(idx >> logN) * NP + P::at(idx & (N - 1))] = zb[u];
+    }
   }
   __syncthreads();
   smem_fft<C, FFT_EPT, false, LOGN>(s, tw);
   // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
   constexpr int half_n = N / 2 + 1;
-#pragma unroll 1
+#pragma unroll 2
   for (int idx = tid; idx < RB * half_n; idx += blockDim.x) {
     int rb = idx / half_n, kk = idx - rb * half_n;
     int j = row0 + rb;
@@ -652,14 +667,26 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   const int k0 = blockIdx.x * CPB;
   const int tid = threadIdx.x;
   const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
-  // gather with the even-first / odd-reversed order (consecutive threads: consecutive columns)
+  // gather with the even-first / odd-reversed order (consecutive threads: consecutive columns);
+  // NT threads (fft_geometry), FFT_EPT values each, loaded in batches of FFT_BATCH
+  constexpr int NT = CPB * h / FFT_EPT;
+  static_assert(NT * FFT_EPT == CPB * h, "columns: whole values per thread");
 #pragma unroll 1
-  for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
-    int j = idx >> logc, cc = idx & (CPB - 1);
-    int k = k0 + cc;
-    C x = k < N ? half[(size_t)j * N + k] : mk<C>((T)0, (T)0);
-    int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
-    s[cc * HP + P::at(pos)] = x;
+  for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
+    C xb[FFT_BATCH];
+#pragma unroll
+    for (int u = 0; u < FFT_BATCH; ++u) {
+      int idx = tid + (q0 + u) * NT;
+      int j = idx >> logc, k = k0 + (idx & (CPB - 1));
+      xb[u] = k < N ? half[(size_t)j * N + k] : mk<C>((T)0, (T)0);
+    }
+#pragma unroll
+    for (int u = 0; u < FFT_BATCH; ++u) {
+      int idx = tid + (q0 + u) * NT;
+      int j = idx >> logc, cc = idx & (CPB - 1);
+      int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
+      s[cc * HP + P::at(pos)] = xb[u];
+    }
   }
   __syncthreads();
   smem_fft<C, FFT_EPT, false, LOGH>(s, tw);
@@ -721,7 +748,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   asm volatile("mov.b64 %0, %1;" : "=l"(tw_inv) : "l"(tw));
   smem_fft<C, FFT_EPT, true, LOGH>(s, tw_inv);
   const T inv_h = (T)1 / (T)h;
-#pragma unroll 1
+#pragma unroll 4
   for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
     int j = idx >> logc, cc = idx & (CPB - 1);
     int k = k0 + cc;
@@ -752,8 +779,27 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   const int row0 = blockIdx.x * RB;
   const int tid = threadIdx.x;
   constexpr int half_n = N / 2 + 1;
+  constexpr int NT = RB * N / FFT_EPT;  // the block's threads (fft_geometry)
+  constexpr int IB = FFT_BATCH / 2;     // pairs (X[k], X[N-k]) loaded per batch
 #pragma unroll 1
-  for (int idx = tid; idx < RB * half_n; idx += blockDim.x) {
+  for (int base = tid; base < RB * half_n; base += IB * NT) {
+    C xkb[IB], xnb[IB];
+#pragma unroll
+    for (int u = 0; u < IB; ++u) {
+      int idx = base + u * NT;
+      int rb = idx / half_n, kk = idx - rb * half_n;
+      int j = row0 + rb;
+      xkb[u] = xnb[u] = mk<C>((T)0, (T)0);
+      if (idx < RB * half_n && j < h) {
+        const C* in = half + (size_t)j * N;
+        xkb[u] = in[kk];
+        if (kk > 0) xnb[u] = in[N - kk];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < IB; ++u) {
+    int idx = base + u * NT;
+    if (idx >= RB * half_n) break;
     int rb = idx / half_n, kk = idx - rb * half_n;
     int j = row0 + rb;
     C* row = s + rb * NP;
@@ -762,13 +808,12 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       if (kk > 0 && kk < N) row[P::at(N - kk)] = mk<C>((T)0, (T)0);
       continue;
     }
-    const C* in = half + (size_t)j * N;
     if (kk == 0) {
-      C p = in[0];  // (X[0], X[N])
+      C p = xkb[u];  // (X[0], X[N])
       row[0] = mk<C>((p.x + p.y) * (T)0.5, (p.x - p.y) * (T)0.5);
       continue;
     }
-    C xk = in[kk], xn = in[N - kk];
+    C xk = xkb[u], xn = xnb[u];
     C E = mk<C>((xk.x + xn.x) * (T)0.5, (xk.y - xn.y) * (T)0.5);
     C D = mk<C>((xk.x - xn.x) * (T)0.5, (xk.y + xn.y) * (T)0.5);
     C O = cmul(D, cconj(post[kk]));
@@ -778,6 +823,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       C O2 = cmul(cconj(D), post[kk]);
       row[P::at(N - kk)] = cadd(cconj(E), cmuli(O2));
     }
+    }
   }
   __syncthreads();
   smem_fft<C, FFT_EPT, true, LOGN>(s, tw);
@@ -785,7 +831,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   Acc<2> acc;
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
-#pragma unroll 1
+#pragma unroll 4
   for (int idx = tid; idx < RB * N; idx += blockDim.x) {
     int rb = idx >> logN, nn = idx & (N - 1);
     int j = row0 + rb;
