@@ -203,11 +203,59 @@ enum {
                   // ||y||^2 into S->rr_true; otherwise nothing
 };
 
-// tiles of 64 x 32 cells (FP32) or 64 x 16 (FP64, to stay inside 48 KB of shared memory), 64 x 4
-// threads
+// tiles of 64 x 32 cells (FP32) or 64 x 16 (FP64), 64 x 4 threads: thread (tx, ty) owns column tx
+// of the tile and a strip of TBY / 4 rows, which it walks with a sliding window of registers
 constexpr int TBX = 64, TTY = 4, TBY_MIN = 16;
 template <class T>
 __host__ __device__ constexpr int tile_rows() { return sizeof(T) == 8 ? 16 : 32; }
+
+// Shared-memory tile rows: local column lc (relative to the tile's first column) sits at offset
+// OFF + lc with OFF = one 16-byte vector, so a row's interior starts on a 16-byte boundary and is
+// staged with 16-byte copies; PITCH holds two halo columns either side, rounded to whole vectors.
+template <class T>
+struct Tile {
+  static constexpr int V = 16 / (int)sizeof(T);
+  static constexpr int OFF = V;
+  static constexpr int PITCH = (OFF + TBX + 2 + V - 1) / V * V;
+};
+
+// Stages local rows [LR0, LR0 + ROWS) (relative to the tile's first row, clamped into [0, h)) and
+// local columns [-HALO, TBX + HALO) (wrapped) of src into dst, row rr at dst + rr * PITCH. With
+// `vec` (a whole tile of 16-byte aligned rows) the interior goes as 16-byte copies and only the
+// halo columns one value at a time.
+template <class T, int ROWS, int HALO, int LR0>
+__device__ __forceinline__ void stage_tile(T* dst, const T* __restrict__ src, int w, int h, int i0, int j0, bool vec,
+                                           int tid) {
+  constexpr int NTH = TBX * TTY;
+  constexpr int V = Tile<T>::V, OFF = Tile<T>::OFF, P = Tile<T>::PITCH;
+  if (vec) {
+    constexpr int VPR = TBX / V;
+    for (int e = tid; e < ROWS * VPR; e += NTH) {
+      int rr = e / VPR, q = e - rr * VPR;
+      int g = min(max(j0 + LR0 + rr, 0), h - 1);
+      __pipeline_memcpy_async(dst + rr * P + OFF + q * V, src + (size_t)g * w + i0 + q * V, 16);
+    }
+    for (int e = tid; e < ROWS * 2 * HALO; e += NTH) {
+      int rr = e / (2 * HALO), hc = e - rr * (2 * HALO);
+      int lc = hc < HALO ? hc - HALO : TBX + hc - HALO;
+      int gc = i0 + lc;
+      gc = gc < 0 ? gc + w : (gc >= w ? gc - w : gc);
+      int g = min(max(j0 + LR0 + rr, 0), h - 1);
+      __pipeline_memcpy_async(dst + rr * P + OFF + lc, src + (size_t)g * w + gc, sizeof(T));
+    }
+  } else {
+    constexpr int RW = TBX + 2 * HALO;
+    for (int e = tid; e < ROWS * RW; e += NTH) {
+      int rr = e / RW, lc = e - rr * RW - HALO;
+      int gc = (i0 + lc) % w;
+      gc = gc < 0 ? gc + w : gc;
+      int g = min(max(j0 + LR0 + rr, 0), h - 1);
+      __pipeline_memcpy_async(dst + rr * P + OFF + lc, src + (size_t)g * w + gc, sizeof(T));
+    }
+  }
+}
+
+__device__ __forceinline__ bool aligned16(const void* p) { return ((size_t)p & 15) == 0; }
 
 template <class T, int MODE>
 __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, const T* __restrict__ v, const T* __restrict__ J,
@@ -222,128 +270,128 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
   }
   if (MODE == RESID_GATED && S->gate_it != S->it) return;
   constexpr bool JAC = MODE == JAC_LEFT || MODE == JAC_FINAL;
-  constexpr int TBY = tile_rows<T>();
-  constexpr int SVR = TBY + 4, SVC = TBX + 4, SMR = TBY + 2, SMC = TBX + 2;
-  // c (and b) are staged with the rest, so the output phase reads nothing from global memory;
-  // the FP64 sandwich reads c directly instead (its tiles would pass the 48 KB of static shared
-  // memory)
-  constexpr bool STAGE_C = MODE != BEND && !(JAC && sizeof(T) == 8);
-  constexpr bool STAGE_B = MODE == RESID || MODE == RESID_GATED;
-  __shared__ T sv[SVR][SVC];                        // the vector, 2-cell halo (JAC: r)
-  __shared__ T sJ[JAC ? SVR : 1][JAC ? SVC : 1];    // JAC: J
-  __shared__ T sP[JAC ? SVR : 1][JAC ? SVC : 1];    // JAC_FINAL: part; then (JAC) u
-  __shared__ T sd[SMR][SMC];                        // d, 1-cell halo; then m = d L v in place
-  __shared__ T sc[STAGE_C ? TBY : 1][STAGE_C ? TBX : 1];  // c on the tile
-  __shared__ T sB[STAGE_B ? TBY : 1][STAGE_B ? TBX : 1];  // b on the tile
+  constexpr bool HAS_B = MODE == RESID || MODE == RESID_GATED;
+  constexpr int TBY = tile_rows<T>(), SEG = TBY / TTY;
+  constexpr int P = Tile<T>::PITCH, OFF = Tile<T>::OFF;
+  constexpr int UR = TBY + 4, MR = TBY + 2;  // vector rows -2 .. TBY + 1; d / m rows -1 .. TBY
+  __shared__ __align__(16) T sv[UR * P];                    // the vector (JAC: r)
+  __shared__ __align__(16) T sJ[JAC ? UR * P : 1];          // JAC: J
+  __shared__ __align__(16) T sP[JAC ? UR * P : 1];          // JAC_FINAL: part; then (JAC) u
+  __shared__ __align__(16) T sd[MR * P];                    // d; then m = d L u in place
   const int i0 = blockIdx.x * TBX, j0 = blockIdx.y * TBY;
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int tid = tx + ty * TBX;
-  auto wrapx = [&](int g) {
-    g %= w;
-    return g < 0 ? g + w : g;
-  };
+  const T* src = JAC ? rb : v;
+  const bool vec = i0 + TBX <= w && (w * (int)sizeof(T)) % 16 == 0 && aligned16(src) && aligned16(d) &&
+                   (!JAC || aligned16(J)) && (MODE != JAC_FINAL || aligned16(part));
   // Stage the tiles with asynchronous copies (every load in flight at once): rows clamp, columns
-  // wrap. Columns tx and, for the first threads, tx + 64 of each tile row.
-  const int ga = wrapx(i0 - 2 + tx), gb = wrapx(i0 - 2 + TBX + tx);
-  const bool extra = tx < SVC - TBX;
-  for (int jj = ty; jj < SVR; jj += TTY) {
-    size_t row = (size_t)min(max(j0 - 2 + jj, 0), h - 1) * w;
-    const T* src = JAC ? rb : v;
-    __pipeline_memcpy_async(&sv[jj][tx], src + row + ga, sizeof(T));
-    if (extra) __pipeline_memcpy_async(&sv[jj][TBX + tx], src + row + gb, sizeof(T));
-    if (JAC) {
-      __pipeline_memcpy_async(&sJ[jj][tx], J + row + ga, sizeof(T));
-      if (extra) __pipeline_memcpy_async(&sJ[jj][TBX + tx], J + row + gb, sizeof(T));
-    }
-    if (MODE == JAC_FINAL) {
-      __pipeline_memcpy_async(&sP[jj][tx], part + row + ga, sizeof(T));
-      if (extra) __pipeline_memcpy_async(&sP[jj][TBX + tx], part + row + gb, sizeof(T));
-    }
-  }
-  const int ma = wrapx(i0 - 1 + tx), mb = wrapx(i0 - 1 + TBX + tx);
-  const bool extra_m = tx < SMC - TBX;
-  for (int mj = ty; mj < SMR; mj += TTY) {
-    size_t row = (size_t)min(max(j0 - 1 + mj, 0), h - 1) * w;
-    __pipeline_memcpy_async(&sd[mj][tx], d + row + ma, sizeof(T));
-    if (extra_m) __pipeline_memcpy_async(&sd[mj][TBX + tx], d + row + mb, sizeof(T));
-  }
-  if (STAGE_C || STAGE_B) {
-    const int ic = i0 + tx;
-    for (int oj = ty; oj < TBY; oj += TTY) {
-      int jc = j0 + oj;
-      if (ic < w && jc < h) {
-        size_t k = (size_t)jc * w + ic;
-        if (STAGE_C) __pipeline_memcpy_async(&sc[oj][tx], c + k, sizeof(T));
-        if (STAGE_B) __pipeline_memcpy_async(&sB[oj][tx], rb + k, sizeof(T));
-      }
-    }
-  }
+  // wrap.
+  stage_tile<T, UR, 2, -2>(sv, src, w, h, i0, j0, vec, tid);
+  if (JAC) stage_tile<T, UR, 2, -2>(sJ, J, w, h, i0, j0, vec, tid);
+  if (MODE == JAC_FINAL) stage_tile<T, UR, 2, -2>(sP, part, w, h, i0, j0, vec, tid);
+  stage_tile<T, MR, 1, -1>(sd, d, w, h, i0, j0, vec, tid);
   __pipeline_commit();
+  // c (and b) for the thread's own output cells, in flight with the tiles
+  const int i = i0 + tx, r0 = ty * SEG;
+  T cr[SEG], br[HAS_B ? SEG : 1];
+#pragma unroll
+  for (int q = 0; q < SEG; ++q) {
+    int j = j0 + r0 + q;
+    bool ok = i < w && j < h;
+    size_t k = (size_t)j * w + i;
+    if (MODE != BEND) cr[q] = ok ? c[k] : (T)0;
+    if (HAS_B) br[q] = ok ? rb[k] : (T)0;
+  }
   __pipeline_wait_prior(0);
   __syncthreads();
   if (JAC) {
     // the vector the mode forms: u = J r (+ part); r and J stay readable for the outputs
-    for (int idx = tid; idx < SVR * SVC; idx += TBX * TTY) {
-      int jj = idx / SVC, ii = idx - jj * SVC;
-      T u = sJ[jj][ii] * sv[jj][ii];
-      if (MODE == JAC_FINAL) u += sP[jj][ii];
-      sP[jj][ii] = u;  // sP now holds u
+    for (int e = tid; e < UR * P; e += TBX * TTY) {
+      T u = sJ[e] * sv[e];
+      if (MODE == JAC_FINAL) u += sP[e];
+      sP[e] = u;
     }
     __syncthreads();
   }
-  T(*su)[SVC] = JAC ? reinterpret_cast<T(*)[SVC]>(&sP[0][0]) : sv;
-  // m = d . L u on the tile plus a 1-cell halo (rows of m clamp the same way)
-  for (int mj = ty; mj < SMR; mj += TTY) {
-    int gm = min(max(j0 - 1 + mj, 0), h - 1);
-    int rn = max(gm - 1, 0) - j0 + 2, rc = gm - j0 + 2, rs = min(gm + 1, h - 1) - j0 + 2;
-    {
-      int mi = tx;
-      T lap = (su[rc][mi] + su[rc][mi + 2] + su[rn][mi + 1] + su[rs][mi + 1] - (T)4 * su[rc][mi + 1]) * inv_dx2;
-      sd[mj][mi] = lap * sd[mj][mi];
-    }
-    if (extra_m) {
-      int mi = TBX + tx;
-      T lap = (su[rc][mi] + su[rc][mi + 2] + su[rn][mi + 1] + su[rs][mi + 1] - (T)4 * su[rc][mi + 1]) * inv_dx2;
-      sd[mj][mi] = lap * sd[mj][mi];
+  const T* su = JAC ? sP : sv;
+  // m = d . L u at local rows -1 .. TBY, columns -1 .. TBX. Column tx over the thread's strip
+  // (the first strip also takes row -1, the last row TBY) with a sliding window down the column.
+  {
+    const int a = r0 - (ty == 0 ? 1 : 0);
+    const T* ucol = su + OFF + tx;  // row lr at (lr + 2) * P
+    T* mcol = sd + OFF + tx;        // row lr at (lr + 1) * P
+    T un = ucol[(a + 1) * P], uc = ucol[(a + 2) * P];
+#pragma unroll
+    for (int q = 0; q < SEG + 1; ++q) {
+      int lr = a + q;
+      if (q == SEG && !(ty == 0 || ty == TTY - 1)) break;
+      T us = ucol[(lr + 3) * P];
+      T lap = (ucol[(lr + 2) * P - 1] + ucol[(lr + 2) * P + 1] + un + us - (T)4 * uc) * inv_dx2;
+      mcol[(lr + 1) * P] = lap * mcol[(lr + 1) * P];
+      un = uc;
+      uc = us;
     }
   }
+  // columns -1 and TBX over all rows
+  for (int e = tid; e < 2 * MR; e += TBX * TTY) {
+    int lr = (e >> 1) - 1, lc = (e & 1) ? TBX : -1;
+    const T* uc = su + (lr + 2) * P + OFF + lc;
+    T lap = (uc[-1] + uc[1] + uc[-P] + uc[P] - (T)4 * uc[0]) * inv_dx2;
+    T* m = sd + (lr + 1) * P + OFF + lc;
+    *m = lap * *m;
+  }
   __syncthreads();
-  T(*sm)[SMC] = sd;
+  // rows of m outside the raster repeat its edge rows (rows clamp): m(-1) = m(0), m(h) = m(h - 1)
+  {
+    const int hb = h - 1 - j0;  // local index of the raster's last row
+    const bool top = j0 == 0, bottom = hb + 1 <= TBY;
+    if (top || bottom) {
+      for (int e = tid; e < TBX + 2; e += TBX * TTY) {
+        if (top) sd[0 * P + OFF - 1 + e] = sd[1 * P + OFF - 1 + e];
+        if (bottom) sd[(hb + 2) * P + OFF - 1 + e] = sd[(hb + 1) * P + OFF - 1 + e];
+      }
+      __syncthreads();
+    }
+  }
   Acc<2> acc;
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
-  const int oi = tx;
-  const int i = i0 + oi;
+  {
+    const T* mcol = sd + OFF + tx;  // m row lr at (lr + 1) * P
+    T mn = mcol[r0 * P], mc = mcol[(r0 + 1) * P];
 #pragma unroll
-  for (int q = 0; q < TBY / TTY; ++q) {
-    int oj = ty + q * TTY;
-    int j = j0 + oj;
-    if (i < w && j < h) {
-      int mn = max(j - 1, 0) - j0 + 1, mc = oj + 1, ms = min(j + 1, h - 1) - j0 + 1;
-      T lm = (sm[mc][oi] + sm[mc][oi + 2] + sm[mn][oi + 1] + sm[ms][oi + 1] - (T)4 * sm[mc][oi + 1]) * inv_dx2;
-      size_t k = (size_t)j * w + i;
-      T u = su[oj + 2][oi + 2];
-      if (MODE == BEND) {
-        y[k] = lm;
-      } else {
-        T au = lm + (STAGE_C ? sc[oj][oi] : c[k]) * u;
-        if (MODE == AP_DOT) {
-          y[k] = au;
-          acc.v[0] += (double)u * (double)au;
-        } else if (MODE == PLAIN) {
-          y[k] = au;
-        } else if (MODE == RESID || MODE == RESID_GATED) {
-          T rr = (STAGE_B ? sB[oj][oi] : rb[k]) - au;
-          y[k] = rr;
-          acc.v[0] += (double)rr * (double)rr;
-        } else if (MODE == JAC_LEFT) {
-          y[k] = sv[oj + 2][oi + 2] - au;
-        } else {  // JAC_FINAL
-          T r = sv[oj + 2][oi + 2];
-          T z = u + sJ[oj + 2][oi + 2] * (r - au);
-          y[k] = z;
-          acc.v[0] += (double)r * (double)z;
-          acc.v[1] = fmax(acc.v[1], fabs((double)z));
+    for (int q = 0; q < SEG; ++q) {
+      const int lr = r0 + q;
+      T ms = mcol[(lr + 2) * P];
+      T lm = (mcol[(lr + 1) * P - 1] + mcol[(lr + 1) * P + 1] + mn + ms - (T)4 * mc) * inv_dx2;
+      mn = mc;
+      mc = ms;
+      int j = j0 + lr;
+      if (i < w && j < h) {
+        size_t k = (size_t)j * w + i;
+        T u = su[(lr + 2) * P + OFF + tx];
+        if (MODE == BEND) {
+          y[k] = lm;
+        } else {
+          T au = lm + cr[q] * u;
+          if (MODE == AP_DOT) {
+            y[k] = au;
+            acc.v[0] += (double)u * (double)au;
+          } else if (MODE == PLAIN) {
+            y[k] = au;
+          } else if (HAS_B) {
+            T rr = br[q] - au;
+            y[k] = rr;
+            acc.v[0] += (double)rr * (double)rr;
+          } else if (MODE == JAC_LEFT) {
+            y[k] = sv[(lr + 2) * P + OFF + tx] - au;
+          } else {  // JAC_FINAL
+            T r = sv[(lr + 2) * P + OFF + tx];
+            T z = u + sJ[(lr + 2) * P + OFF + tx] * (r - au);
+            y[k] = z;
+            acc.v[0] += (double)r * (double)z;
+            acc.v[1] = fmax(acc.v[1], fabs((double)z));
+          }
         }
       }
     }
