@@ -414,6 +414,12 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
 // ---------------------------------------------------------------------------------------------
 // CG vector kernels (grid-stride).
 
+// 16 bytes of T: the vector kernels move whole 16-byte words (the handle's buffers are aligned)
+template <class T>
+struct alignas(16) Vec16 {
+  T a[16 / sizeof(T)];
+};
+
 // x += alpha p; r -= alpha Ap; reduce r.r
 template <class T>
 __global__ void __launch_bounds__(256) k_update(size_t n, T* __restrict__ x, T* __restrict__ r, const T* __restrict__ p,
@@ -422,14 +428,33 @@ __global__ void __launch_bounds__(256) k_update(size_t n, T* __restrict__ x, T* 
     if (blockIdx.x == 0 && threadIdx.x == 0) set_cond(S, 0);
     return;
   }
+  constexpr int V = 16 / sizeof(T);
+  using W = Vec16<T>;
   T alpha = (T)S->alpha;
   Acc<1> acc;
   acc.v[0] = 0.0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+  const size_t nv = n / V, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  W* xv = reinterpret_cast<W*>(x);
+  W* rv = reinterpret_cast<W*>(r);
+  const W* pv = reinterpret_cast<const W*>(p);
+  const W* av = reinterpret_cast<const W*>(ap);
+  for (size_t kv = t0; kv < nv; kv += stride) {
+    W xx = xv[kv], rr = rv[kv], pp = pv[kv], aa = av[kv];
+#pragma unroll
+    for (int e = 0; e < V; ++e) {
+      xx.a[e] += alpha * pp.a[e];
+      rr.a[e] = rr.a[e] - alpha * aa.a[e];
+      acc.v[0] += (double)rr.a[e] * (double)rr.a[e];
+    }
+    xv[kv] = xx;
+    rv[kv] = rr;
+  }
+  for (size_t k = nv * V + t0; k < n; k += stride) {
     x[k] += alpha * p[k];
-    T rv = r[k] - alpha * ap[k];
-    r[k] = rv;
-    acc.v[0] += (double)rv * (double)rv;
+    T rk = r[k] - alpha * ap[k];
+    r[k] = rk;
+    acc.v[0] += (double)rk * (double)rk;
   }
   const int kind[1] = {0};
   if (reduce_partials<1>(acc, kind, partials, &S->ticket[SITE_UPDATE], gridDim.x) && threadIdx.x == 0) finish_update(S, acc.v[0]);
@@ -446,9 +471,20 @@ __global__ void __launch_bounds__(256) k_direction(size_t n, T* __restrict__ p, 
     set_cond(S, again ? 1u : 0u);
   }
   if (S->stop) return;
+  constexpr int V = 16 / sizeof(T);
+  using W = Vec16<T>;
   T beta = (T)S->beta;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    p[k] = z[k] + beta * p[k];
+  const size_t nv = n / V, stride = (size_t)gridDim.x * blockDim.x;
+  const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  W* pv = reinterpret_cast<W*>(p);
+  const W* zv = reinterpret_cast<const W*>(z);
+  for (size_t kv = t0; kv < nv; kv += stride) {
+    W pp = pv[kv], zz = zv[kv];
+#pragma unroll
+    for (int e = 0; e < V; ++e) pp.a[e] = zz.a[e] + beta * pp.a[e];
+    pv[kv] = pp;
+  }
+  for (size_t k = nv * V + t0; k < n; k += stride) p[k] = z[k] + beta * p[k];
 }
 
 template <class A, class B>
