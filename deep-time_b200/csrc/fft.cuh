@@ -8,7 +8,8 @@
 // synchronises, every thread writes its outputs. A block transforms `batch` sequences of length N;
 // each thread holds EPT (8 or 16) complex values per stage, so the block has batch * N / EPT
 // threads. Twiddles come from a table tw[t] = e^(-2 pi i t / N) built on the host (long double
-// angles); the inverse transform (unnormalised) conjugates them.
+// angles); the inverse transform (unnormalised) conjugates them. A stage loads w^1, w^2, w^4, w^8
+// and forms the other powers by products.
 //
 // Shared-memory layout: element i of a sequence lives at pad(i) = i + (i >> 4), one spare slot
 // after every 16 values. The first stage's writes (stride 16) then fall in distinct banks for
@@ -140,12 +141,24 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
 #pragma unroll
     for (int r = 0; r < R; ++r) v[q][r] = base[Pad<C>::at(j + r * NBF)];
     if (NS > 1) {
+      // w^r for r = 1 .. R-1 from the table's w, w^2, w^4, w^8 and products of those (at most
+      // three roundings from exact values): four table loads instead of R - 1
+      C w[R];
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        C w = tw[r * STEP * k];
-        if (INV) w.y = -w.y;
-        v[q][r] = cmul(v[q][r], w);
+      for (int p2 = 1; p2 < R; p2 *= 2) {
+        C t = tw[p2 * STEP * k];
+        if (INV) t.y = -t.y;
+        w[p2] = t;
       }
+#pragma unroll
+      for (int r = 3; r < R; ++r) {
+        if ((r & (r - 1)) == 0) continue;
+        int hi = 1;
+        while (hi * 2 <= r) hi *= 2;
+        w[r] = cmul(w[r - hi], w[hi]);
+      }
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], w[r]);
     }
     obase[q] = b * NP;
     oidx[q] = (j - k) * R + k;
