@@ -784,17 +784,18 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
     C* col = s + cc * HP;
     // divisors: column 0 is packed (real part k = 0, imaginary part k = N)
     // 1 / (d lambda^2 + c): one reciprocal per divisor, then products
-    auto rden = [&](int kx, int mm) {
-      T l = (lx[kx] + ly[mm]) * inv_dx2;
+    auto rden = [&](int kx, T lyv) {
+      T l = (lx[kx] + lyv) * inv_dx2;
       return recip(dref * (l * l) + cref);
     };
+    const T lym = ly[m];
     if (m == 0) {
       C v0 = col[0];
       if (k == 0) {
-        v0.x *= rden(0, 0);
-        v0.y *= rden(N, 0);
+        v0.x *= rden(0, lym);
+        v0.y *= rden(N, lym);
       } else {
-        T dd = rden(k, 0);
+        T dd = rden(k, lym);
         v0.x *= dd;
         v0.y *= dd;
       }
@@ -803,25 +804,28 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
     }
     int mm = h - m;
     int pm = P::at(m), pn = P::at(mm);
-    C p = cmul(omega[m], col[pm]);
-    C q = cmul(omega[mm], col[pn]);
+    // w_(h-m) = -i conj(w_m) and ly[h-m] = -ly[m] - 4 (cos(pi - t) = -cos t): one table entry each
+    const C wm = omega[m], wn = mk<C>(-wm.y, -wm.x);
+    const T lyn = -lym - (T)4;
+    C p = cmul(wm, col[pm]);
+    C q = cmul(wn, col[pn]);
     C cm = cscale(cadd(p, cmuli(q)), (T)0.5);
     C cn = cscale(cadd(q, cmuli(p)), (T)0.5);
     if (k == 0) {
-      cm.x *= rden(0, m);
-      cm.y *= rden(N, m);
-      cn.x *= rden(0, mm);
-      cn.y *= rden(N, mm);
+      cm.x *= rden(0, lym);
+      cm.y *= rden(N, lym);
+      cn.x *= rden(0, lyn);
+      cn.y *= rden(N, lyn);
     } else {
-      T a = rden(k, m), b = rden(k, mm);
+      T a = rden(k, lym), b = rden(k, lyn);
       cm.x *= a;
       cm.y *= a;
       cn.x *= b;
       cn.y *= b;
     }
     // V'[m] = conj(w_m) (C[m] - i C[h-m])
-    C vm = cmul(cconj(omega[m]), csub(cm, cmuli(cn)));
-    C vn = cmul(cconj(omega[mm]), csub(cn, cmuli(cm)));
+    C vm = cmul(cconj(wm), csub(cm, cmuli(cn)));
+    C vn = cmul(cconj(wn), csub(cn, cmuli(cm)));
     col[pm] = vm;
     if (mm != m) col[pn] = vn;
   }
