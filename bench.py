@@ -67,7 +67,7 @@ def parse():
     ap.add_argument("--case", default=None,
                     help="profiling aid (for ncu): run one host-driven, iteration-capped solve and exit; "
                          "'W,H,DX,PRECOND,PRECISION,ITERATIONS' with PRECOND 0 reference / 1 mean-D and PRECISION "
-                         "0 fp64 / 1 mixed")
+                         "0 fp64 / 1 FP32 inside FP64 refinement / 2 FP32 with FP64 reliable updates")
     return ap.parse_args()
 
 
