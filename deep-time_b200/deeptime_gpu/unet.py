@@ -183,6 +183,16 @@ def flexure_problem_torch(w, h, sigma, seed, device, topo_std=1500.0, beta=2.0):
     return D / G, torch.full((h, w), C_MANTLE, dtype=torch.float64, device=device), 2700.0 * topo
 
 
+def diffusion_problem_torch(w, h, sigma, seed, device, topo_std=800.0, beta=2.5):
+    """inputs.diffusion_problem on the device: (h0, s) float64 tensors, s = kappa dt / dx^2 a
+    smoothed log-uniform field over [0.1, 100]."""
+    topo = _grf(w, h, beta, topo_std, seed, device)
+    v = _smooth(splitmix_f64_torch(seed + 1, w * h, device).reshape(h, w), sigma)
+    lo, hi = v.min(), v.max()
+    v = (v - lo) / (hi - lo)
+    return topo, 10.0 ** (-1.0 + 3.0 * v)
+
+
 def normalise_inputs(d, b, c_mean=C_MANTLE):
     """(x [h][w][2] float32, scale) with scale = rms(b) / c_mean, so that w = prediction * scale."""
     import torch

@@ -238,3 +238,19 @@ def test_the_iteration_cap_reports_not_converged():
     x, rep = F.Solver(w, h, dx).solve_with(d, c, b, F.params(precond=L.PRECOND_MEAN_D, stop=L.STOP_REL_RESIDUAL,
                                                               tol=1e-14, max_iterations=3))
     assert not rep.converged and rep.iterations == 3 and rep.status == L.DT_NOT_CONVERGED
+
+
+@pytest.mark.parametrize("precision", [L.PREC_FP64, L.PREC_MIXED])
+@pytest.mark.parametrize("w,h", [(16384, 64), (128, 8192)])
+def test_the_longest_transforms_match_the_oracle(w, h, precision):
+    # rows of 8192 complex values (w = 16384) and columns of 8192: the lengths of the 16384 x 8192
+    # timestep raster, on thin rasters the oracle solves in seconds
+    dx = 1250.0
+    d, c, _ = I.flexure_problem(w, h, 8.0, 77)
+    r = np.random.default_rng(w).standard_normal((h, w)) * 1e4
+    sv = F.Solver(w, h, dx)
+    for precond in (L.PRECOND_MEAN_D, L.PRECOND_REFERENCE):
+        z = sv.precondition(d, c, r, precond, precision)
+        want = O.flex_precondition(d, c, r, dx, precond)
+        bound = (1e-12 if precond == L.PRECOND_MEAN_D else 1e-8) if precision == L.PREC_FP64 else 5e-5
+        assert rel_l2(z, want) < bound, (precond, rel_l2(z, want))
