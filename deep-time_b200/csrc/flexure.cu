@@ -78,6 +78,8 @@ struct Scalars {
   int gate_it;
   double delta2, maxrr;
   double rr_true, bb_true;  // ||b - A x||^2 and ||b||^2 in FP64, unscaled
+  int replacements;         // residual replacements so far
+  unsigned long long cond_if;  // the loop body's IF node around the replacement, 0 without one
 };
 
 __device__ __forceinline__ void set_cond(Scalars* S, unsigned int v) {
@@ -102,13 +104,16 @@ __device__ void finish_update(Scalars* S, double rr) {
   S->it += 1;
   if (S->reliable) {
     // the sloppy residual only asks for a replacement; the FP64 residual decides convergence
+    bool gate = false;
     if (!isfinite(rr)) {
       S->stop = STOP_NONFINITE;
     } else if (rr <= S->tol * S->tol * S->bb || rr < S->delta2 * S->maxrr) {
       S->gate_it = S->it;
+      gate = true;
     } else if (S->it >= S->max_it) {
       S->stop = STOP_CAP;
     }
+    if (S->cond_if) cudaGraphSetConditional((cudaGraphConditionalHandle)S->cond_if, gate ? 1u : 0u);
     if (S->stop) set_cond(S, 0);
     return;
   }
@@ -535,6 +540,7 @@ __global__ void k_reliable_reset(size_t n, const double* __restrict__ r, float* 
     double rr = S->rr_true * sc * sc;
     S->rr = rr;
     S->maxrr = rr;
+    S->replacements += 1;
     if (!isfinite(S->rr_true)) {
       S->stop = STOP_NONFINITE;
     } else if (S->rr_true <= S->tol * S->tol * S->bb_true) {
@@ -561,6 +567,8 @@ __global__ void k_reliable_init(Scalars* F, const Scalars* S64, const double* sc
   F->delta2 = delta * delta;
   F->gate_it = -1;
   F->reliable = 1;
+  F->replacements = 0;
+  F->cond_if = 0ull;
 }
 
 template <class T>
@@ -954,12 +962,16 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
 
 // Before the loop: give the scalars the graph's conditional handle and run the body only when
 // nothing has stopped the solve yet.
-__global__ void k_arm(Scalars* S, unsigned long long handle) {
+__global__ void k_arm(Scalars* S, unsigned long long handle, unsigned long long handle_if) {
   S->cond = handle;
+  S->cond_if = handle_if;
   S->body_runs = 0;
   cudaGraphSetConditional((cudaGraphConditionalHandle)handle, S->stop == 0 ? 1u : 0u);
 }
-__global__ void k_disarm(Scalars* S) { S->cond = 0ull; }
+__global__ void k_disarm(Scalars* S) {
+  S->cond = 0ull;
+  S->cond_if = 0ull;
+}
 
 // A fresh solve state (keeps the problem fields, the bank and the handle slot cleared).
 __global__ void k_reset(Scalars* S) {
@@ -1326,18 +1338,64 @@ static void launch_reliable(dt_flex* s, cudaStream_t st) {
   k_reliable_reset<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, s->scale, F.S); counted();
 }
 
+// While `st` captures a loop body: a conditional IF node, its body the residual replacement
+// (captured on `aside`), so that iterations that replace nothing launch nothing for it. The
+// update's finisher sets the node's condition. The replacement's kernels are left out of the
+// body's launch count (a solve counts them from S->replacements).
+static dt_status add_reliable_if(dt_flex* s, cudaStream_t st, cudaStream_t aside, unsigned long long* handle_out) {
+  cudaStreamCaptureStatus cs;
+  unsigned long long id = 0;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  DT_CUDA(cudaStreamGetCaptureInfo(st, &cs, &id, &graph, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive || !graph) {
+    set_error("flexure loop graph: the stream is not capturing");
+    return DT_DEVICE_ERROR;
+  }
+  cudaGraphConditionalHandle h;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  DT_CUDA(cudaGraphAddNode(&node, graph, deps, nd, &cp));
+  DT_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  long long kept = g_captured;
+  DT_CUDA(cudaStreamBeginCaptureToGraph(aside, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+  launch_reliable(s, aside);
+  cudaGraph_t ifbody;
+  DT_CUDA(cudaStreamEndCapture(aside, &ifbody));
+  g_captured = kept;
+  *handle_out = (unsigned long long)h;
+  return DT_OK;
+}
+
 // One PCG iteration (flexure.rs:1709-1738): the body of the device loop. With `reliable` (FP32
 // lane) the residual replacement sits between the update and the preconditioner, so z, beta and
-// p follow the replaced residual and the search direction carries on.
+// p follow the replaced residual and the search direction carries on. Driven from the host its
+// kernels run every iteration and do nothing unless gated on; in the graph (`aside` given) they
+// sit in an IF node.
 template <class T>
-static void launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st, bool reliable = false) {
+static dt_status launch_iteration(dt_flex* s, Lane<T>& L, int levels, cudaStream_t st, bool reliable = false,
+                                  cudaStream_t aside = nullptr, unsigned long long* if_handle = nullptr) {
   launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st);
   k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); counted();
   if constexpr (sizeof(T) == 4) {
-    if (reliable) launch_reliable(s, st);
+    if (reliable) {
+      if (aside) {
+        DT_TRY(add_reliable_if(s, st, aside, if_handle));
+      } else {
+        launch_reliable(s, st);
+      }
+    }
   }
   launch_precondition<T>(s, L, L.r, L.z, levels, st);
   k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); counted();
+  return DT_OK;
 }
 
 // The loop graph: k_arm -> WHILE(iteration) -> k_disarm. Built once per lane and level count.
@@ -1352,10 +1410,10 @@ static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* 
   DT_CUDA(cudaGraphCreate(&g, 0));
   cudaGraphConditionalHandle handle;
   DT_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
-  unsigned long long hv = (unsigned long long)handle;
+  unsigned long long hv = (unsigned long long)handle, hv_if = 0ull;
   Scalars* Sp = L.S;
   cudaKernelNodeParams kp = {};
-  void* arm_args[] = {&Sp, &hv};
+  void* arm_args[] = {&Sp, &hv, &hv_if};
   kp.func = (void*)k_arm;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(1);
@@ -1369,14 +1427,20 @@ static dt_status loop_exec(dt_flex* s, Lane<T>& L, int levels, cudaGraphExec_t* 
   cp.conditional.size = 1;
   DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t aside = nullptr;
+  if (reliable) DT_CUDA(cudaStreamCreateWithFlags(&aside, cudaStreamNonBlocking));
   DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   g_capturing = true;
   g_captured = 0;
-  launch_iteration<T>(s, L, levels, s->stream, reliable);
+  dt_status st_body = launch_iteration<T>(s, L, levels, s->stream, reliable, aside, &hv_if);
   g_capturing = false;
   L.body_kernels[li] = g_captured;
   cudaGraph_t captured;
-  DT_CUDA(cudaStreamEndCapture(s->stream, &captured));
+  cudaError_t e_end = cudaStreamEndCapture(s->stream, &captured);
+  if (aside) cudaStreamDestroy(aside);
+  DT_TRY(st_body);
+  DT_CUDA(e_end);
+  if (reliable) DT_CUDA(cudaGraphKernelNodeSetParams(n_arm, &kp));  // k_arm learns the IF node's handle
   void* dis_args[] = {&Sp};
   kp.func = (void*)k_disarm;
   kp.kernelParams = dis_args;
@@ -1448,7 +1512,7 @@ static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop, bool
   Scalars h;
   DT_TRY(read_scalars(s, L.S, &h));
   for (int pass = 0; pass < h.max_it + 2 && h.stop == STOP_RUNNING; ++pass) {
-    launch_iteration<T>(s, L, levels, st, reliable);
+    DT_TRY(launch_iteration<T>(s, L, levels, st, reliable));
     DT_CUDA(cudaGetLastError());
     DT_TRY(read_scalars(s, L.S, &h));
     if (host_loop > 1)
@@ -1699,6 +1763,7 @@ static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool 
   Scalars h, hf;
   DT_TRY(read_scalars(s, F.S, &hf));
   count_loop(F, levels, p->host_loop, hf.body_runs, true);
+  if (!p->host_loop) g_launches += 3LL * hf.replacements;  // the IF node's kernels, when they ran
   DT_TRY(read_scalars(s, L.S, &h));
   bool nonfinite = hf.stop == STOP_NONFINITE || !std::isfinite(h.rr) || !std::isfinite(h.bb);
   double bref = p->stop == DT_STOP_RMS_RESIDUAL ? (double)s->n : h.bb;
