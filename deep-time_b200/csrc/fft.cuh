@@ -18,11 +18,6 @@
 #pragma once
 #include "common.cuh"
 
-// The largest radix the stages use (16 or 8); a build option for comparing the two.
-#ifndef DT_FFT_MAX_RADIX
-#define DT_FFT_MAX_RADIX 16
-#endif
-
 namespace dt {
 
 template <class C>
@@ -117,13 +112,46 @@ __device__ __forceinline__ void dft16(C* v) {
   }
 }
 
+// w^r (r = 1 .. R-1) of w = tw[base] (conjugated for the inverse): the table's w, w^2, w^4, w^8
+// and products of those (at most three roundings from exact values), four loads instead of R - 1.
+template <class C, int R, bool INV>
+__device__ __forceinline__ void stage_twiddles(const C* __restrict__ tw, int base, C* w) {
+#pragma unroll
+  for (int p2 = 1; p2 < R; p2 *= 2) {
+    C t = tw[p2 * base];
+    if (INV) t.y = -t.y;
+    w[p2] = t;
+  }
+#pragma unroll
+  for (int r = 3; r < R; ++r) {
+    if ((r & (r - 1)) == 0) continue;
+    int hi = 1;
+    while (hi * 2 <= r) hi *= 2;
+    w[r] = cmul(w[r - hi], w[hi]);
+  }
+}
+
+// The length-R DFT of v in place.
+template <class C, int R, bool INV>
+__device__ __forceinline__ void dft_r(C* v) {
+  if constexpr (R == 16) {
+    dft16<C, INV>(v);
+  } else if constexpr (R == 8) {
+    dft8<C, INV>(v);
+  } else if constexpr (R == 4) {
+    dft4<C, INV>(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 2) {
+    dft2<C, INV>(v[0], v[1]);
+  }
+}
+
 // One stage of radix R over the block's sequences of length N = 2^LOGN, each stored at
 // s + b * NP (padded); span NS. Everything but the data is known at compile time, so the index
 // arithmetic is shifts and masks. Threads: batch * N / EPT, each owns EPT / R butterflies.
-template <class C, int R, int EPT, bool INV, int LOGN, int NS>
+template <class C, int R, int EPT, bool INV, int LOGN, int NS, int PITCH = 0>
 __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   constexpr int N = 1 << LOGN;
-  constexpr int NP = Pad<C>::len(N);
+  constexpr int NP = PITCH ? PITCH : Pad<C>::len(N);
   constexpr int B = EPT / R;
   constexpr int NBF = N / R;
   constexpr int LOGNBF = LOGN - (R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1);
@@ -141,22 +169,8 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
 #pragma unroll
     for (int r = 0; r < R; ++r) v[q][r] = base[Pad<C>::at(j + r * NBF)];
     if (NS > 1) {
-      // w^r for r = 1 .. R-1 from the table's w, w^2, w^4, w^8 and products of those (at most
-      // three roundings from exact values): four table loads instead of R - 1
       C w[R];
-#pragma unroll
-      for (int p2 = 1; p2 < R; p2 *= 2) {
-        C t = tw[p2 * STEP * k];
-        if (INV) t.y = -t.y;
-        w[p2] = t;
-      }
-#pragma unroll
-      for (int r = 3; r < R; ++r) {
-        if ((r & (r - 1)) == 0) continue;
-        int hi = 1;
-        while (hi * 2 <= r) hi *= 2;
-        w[r] = cmul(w[r - hi], w[hi]);
-      }
+      stage_twiddles<C, R, INV>(tw, STEP * k, w);
 #pragma unroll
       for (int r = 1; r < R; ++r) v[q][r] = cmul(v[q][r], w[r]);
     }
@@ -166,15 +180,7 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   __syncthreads();
 #pragma unroll
   for (int q = 0; q < B; ++q) {
-    if (R == 16) {
-      dft16<C, INV>(v[q]);
-    } else if (R == 8) {
-      dft8<C, INV>(v[q]);
-    } else if (R == 4) {
-      dft4<C, INV>(v[q][0], v[q][1], v[q][2], v[q][3]);
-    } else {
-      dft2<C, INV>(v[q][0], v[q][1]);
-    }
+    dft_r<C, R, INV>(v[q]);
 #pragma unroll
     for (int r = 0; r < R; ++r) s[obase[q] + Pad<C>::at(oidx[q] + r * NS)] = v[q][r];
   }
@@ -183,22 +189,27 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
 
 // Stages from span NS on: radix 16 while four or more factors of two remain (and a thread holds
 // 16 values), then 8, 4 or 2.
-template <class C, int EPT, bool INV, int LOGN, int NS, int REM>
+template <class C, int EPT, bool INV, int LOGN, int NS, int REM, int PITCH = 0>
 struct Stages {
   static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
-    if constexpr (REM >= 4 && EPT % 16 == 0 && DT_FFT_MAX_RADIX >= 16) {
-      stockham_stage<C, 16, EPT, INV, LOGN, NS>(s, tw);
-      Stages<C, EPT, INV, LOGN, NS * 16, REM - 4>::run(s, tw);
+    if constexpr (REM >= 4 && EPT % 16 == 0) {
+      stockham_stage<C, 16, EPT, INV, LOGN, NS, PITCH>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 16, REM - 4, PITCH>::run(s, tw);
     } else if constexpr (REM >= 3) {
-      stockham_stage<C, 8, EPT, INV, LOGN, NS>(s, tw);
-      Stages<C, EPT, INV, LOGN, NS * 8, REM - 3>::run(s, tw);
+      stockham_stage<C, 8, EPT, INV, LOGN, NS, PITCH>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 8, REM - 3, PITCH>::run(s, tw);
     } else if constexpr (REM == 2) {
-      stockham_stage<C, 4, EPT, INV, LOGN, NS>(s, tw);
+      stockham_stage<C, 4, EPT, INV, LOGN, NS, PITCH>(s, tw);
     } else if constexpr (REM == 1) {
-      stockham_stage<C, 2, EPT, INV, LOGN, NS>(s, tw);
+      stockham_stage<C, 2, EPT, INV, LOGN, NS, PITCH>(s, tw);
     }
   }
 };
+
+// The radix the stages above give a length-2^LOGN transform's last stage.
+__host__ __device__ constexpr int last_radix(int logn) {
+  return logn % 4 == 0 ? 16 : (1 << (logn % 4));
+}
 
 // Full transform of length 2^LOGN. The caller synchronises before (data in s) and may read s
 // after it returns.

@@ -663,9 +663,15 @@ constexpr int FFT_MAX_THREADS = 512;
 __host__ __device__ constexpr int rows_per_block(int logn) { return (32 * FFT_EPT >> logn) > 1 ? (32 * FFT_EPT >> logn) : 1; }
 // Columns per block of the column pass: at least one warp, at most FFT_MAX_THREADS threads,
 // 100 KB of padded shared memory, 8 columns.
+// Column pitch of the column pass: the padded length rounded up to 4 (mod 16), so that the first
+// and last stages' interleaved accesses (CPB columns x consecutive rows) fall in distinct banks.
+__host__ __device__ constexpr int col_pitch(int h) {
+  int l = h + (h >> 4) + 1;
+  return l + ((4 - l % 16) + 16) % 16;
+}
 __host__ __device__ constexpr int cols_per_block(int logh, int elem) {
   int h = 1 << logh;
-  int plen = h + (h >> 4) + 1;
+  int plen = col_pitch(h);
   int cpb = (32 * FFT_EPT >> logh) > 1 ? (32 * FFT_EPT >> logh) : 1;
   while (cpb < 8 && cpb * 2 * h <= FFT_MAX_THREADS * FFT_EPT && cpb * 2 * plen * elem <= 102400) cpb *= 2;
   return cpb;
@@ -753,35 +759,54 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   constexpr int h = 1 << LOGH;
-  constexpr int HP = P::len(h);
+  constexpr int HP = col_pitch(h);
   constexpr int CPB = cols_per_block(LOGH, (int)sizeof(C));
   constexpr int logc = CPB == 1 ? 0 : CPB == 2 ? 1 : CPB == 4 ? 2 : CPB == 8 ? 3 : CPB == 16 ? 4 : CPB == 32 ? 5 : CPB == 64 ? 6 : CPB == 128 ? 7 : 8;
   const int k0 = blockIdx.x * CPB;
   const int tid = threadIdx.x;
   const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
-  // gather with the even-first / odd-reversed order (consecutive threads: consecutive columns);
-  // NT threads (fft_geometry), FFT_EPT values each, loaded in batches of FFT_BATCH
+  // NT threads (fft_geometry), FFT_EPT values each
   constexpr int NT = CPB * h / FFT_EPT;
   static_assert(NT * FFT_EPT == CPB * h, "columns: whole values per thread");
+  // Makhoul's order: v[p] = x[2p] for p < h/2, x[2(h - 1 - p) + 1] after
+  auto row_of = [](int p) { return p < h / 2 ? 2 * p : 2 * (h - 1 - p) + 1; };
+  if constexpr (LOGH < 4) {
+    // short columns: gather in Makhoul's order (consecutive threads: consecutive columns)
 #pragma unroll 1
-  for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
-    C xb[FFT_BATCH];
+    for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
+      C xb[FFT_BATCH];
 #pragma unroll
-    for (int u = 0; u < FFT_BATCH; ++u) {
-      int idx = tid + (q0 + u) * NT;
-      int j = idx >> logc, k = k0 + (idx & (CPB - 1));
-      xb[u] = k < N ? half[(size_t)j * N + k] : mk<C>((T)0, (T)0);
-    }
+      for (int u = 0; u < FFT_BATCH; ++u) {
+        int idx = tid + (q0 + u) * NT;
+        int j = idx >> logc, k = k0 + (idx & (CPB - 1));
+        xb[u] = k < N ? half[(size_t)j * N + k] : mk<C>((T)0, (T)0);
+      }
 #pragma unroll
-    for (int u = 0; u < FFT_BATCH; ++u) {
-      int idx = tid + (q0 + u) * NT;
-      int j = idx >> logc, cc = idx & (CPB - 1);
-      int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
-      s[cc * HP + P::at(pos)] = xb[u];
+      for (int u = 0; u < FFT_BATCH; ++u) {
+        int idx = tid + (q0 + u) * NT;
+        int j = idx >> logc, cc = idx & (CPB - 1);
+        int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
+        s[cc * HP + P::at(pos)] = xb[u];
+      }
     }
+    __syncthreads();
+    Stages<C, FFT_EPT, false, LOGH, 1, LOGH, HP>::run(s, tw);
+  } else {
+    // The forward transform's first stage (radix 16, span 1) straight from global memory: thread
+    // tid takes butterfly j = tid / CPB of column tid % CPB, i.e. v[j + r h/16], r = 0 .. 15; a
+    // warp reads 32-byte row segments of CPB columns.
+    const int cc = tid & (CPB - 1), j = tid >> logc, k = k0 + cc;
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+      v[r] = k < N ? half[(size_t)row_of(j + r * (h / 16)) * N + k] : mk<C>((T)0, (T)0);
+    dft_r<C, 16, false>(v);
+    C* col = s + cc * HP;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) col[P::at(j * 16 + r)] = v[r];
+    __syncthreads();
+    Stages<C, FFT_EPT, false, LOGH, 16, LOGH - 4, HP>::run(s, tw);
   }
-  __syncthreads();
-  smem_fft<C, FFT_EPT, false, LOGH>(s, tw);
   // per column and pair (m, h - m): C[m] = (w_m V[m] + i w_(h-m) V[h-m]) / 2, divide, and back
   constexpr int half_h = h / 2 + 1;
 #pragma unroll 1
@@ -842,15 +867,45 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   // the forward stages' twiddles in registers for the inverse stages and spills
   const C* tw_inv;
   asm volatile("mov.b64 %0, %1;" : "=l"(tw_inv) : "l"(tw));
-  smem_fft<C, FFT_EPT, true, LOGH>(s, tw_inv);
   const T inv_h = (T)1 / (T)h;
+  if constexpr (LOGH < 4) {
+    Stages<C, FFT_EPT, true, LOGH, 1, LOGH, HP>::run(s, tw_inv);
 #pragma unroll 4
-  for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
-    int j = idx >> logc, cc = idx & (CPB - 1);
-    int k = k0 + cc;
-    if (k >= N) continue;
-    int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
-    half[(size_t)j * N + k] = cscale(s[cc * HP + P::at(pos)], inv_h);
+    for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
+      int j = idx >> logc, cc = idx & (CPB - 1);
+      int k = k0 + cc;
+      if (k >= N) continue;
+      int pos = (j & 1) ? h - 1 - (j >> 1) : (j >> 1);
+      half[(size_t)j * N + k] = cscale(s[cc * HP + P::at(pos)], inv_h);
+    }
+  } else {
+    // all stages but the last through shared memory; the last (radix RL, span h / RL, twiddles
+    // w^(r j)) writes each output straight to its row of the half spectrum, CPB columns per
+    // 32-byte segment
+    constexpr int RL = last_radix(LOGH);
+    constexpr int LOGRL = RL == 16 ? 4 : RL == 8 ? 3 : RL == 4 ? 2 : 1;
+    constexpr int NSL = h / RL;
+    Stages<C, FFT_EPT, true, LOGH, 1, LOGH - LOGRL, HP>::run(s, tw_inv);
+#pragma unroll
+    for (int q = 0; q < FFT_EPT / RL; ++q) {
+      const int u = tid + q * NT;
+      const int cc = u & (CPB - 1), j = u >> logc, k = k0 + cc;
+      const C* col = s + cc * HP;
+      C v[RL];
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[r] = col[P::at(j + r * NSL)];
+      if (NSL > 1) {
+        C w[RL];
+        stage_twiddles<C, RL, true>(tw_inv, j, w);
+#pragma unroll
+        for (int r = 1; r < RL; ++r) v[r] = cmul(v[r], w[r]);
+      }
+      dft_r<C, RL, true>(v);
+      if (k < N) {
+#pragma unroll
+        for (int r = 0; r < RL; ++r) half[(size_t)row_of(j + r * NSL) * N + k] = cscale(v[r], inv_h);
+      }
+    }
   }
 }
 
@@ -1227,7 +1282,7 @@ static FftGeo fft_geometry(const dt_flex* s) {
   int cpb = cols_per_block(logh, (int)sizeof(C));
   g.cgrid = ceil_div(N, cpb);
   g.cthreads = std::max(1, cpb * s->h / FFT_EPT);
-  g.csmem = (size_t)cpb * Pad<C>::len(s->h) * sizeof(C);
+  g.csmem = (size_t)cpb * col_pitch(s->h) * sizeof(C);
   return g;
 }
 
