@@ -696,34 +696,59 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   // stores so that a thread keeps FFT_BATCH of them in flight.
   constexpr int NT = RB * N / FFT_EPT;
   static_assert(NT * FFT_EPT == RB * N, "rows: whole pairs per thread");
-#pragma unroll 1
-  for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
-    C zb[FFT_BATCH];
+  if constexpr (RB == 1 && LOGN >= 4) {
+    // one row per block: the first stage (radix 16, span 1) straight from global memory, thread
+    // j taking pairs n = j + r N/16 (consecutive threads, consecutive pairs)
+    const int j = tid;
+    C z[16];
 #pragma unroll
-    for (int u = 0; u < FFT_BATCH; ++u) {
-      int idx = tid + (q0 + u) * NT;
-      int rb = idx >> logN, nn = idx & (N - 1);
-      int j = row0 + rb;
-      C z = mk<C>((T)0, (T)0);
-      if (j < h) {
-        size_t k = (size_t)j * w + 2 * nn;
-        z = *reinterpret_cast<const C*>(v + k);
+    for (int r = 0; r < 16; ++r) {
+      z[r] = mk<C>((T)0, (T)0);
+      if (row0 < h) {
+        size_t k = (size_t)row0 * w + 2 * (j + r * (N / 16));
+        z[r] = *reinterpret_cast<const C*>(v + k);
         if (WEIGHT) {
           C ww = *reinterpret_cast<const C*>(wt + k);
-          z.x *= ww.x;
-          z.y *= ww.y;
+          z[r].x *= ww.x;
+          z[r].y *= ww.y;
         }
       }
-      zb[u] = z;
     }
+    dft_r<C, 16, false>(z);
 #pragma unroll
-    for (int u = 0; u < FFT_BATCH; ++u) {
-      int idx = tid + (q0 + u) * NT;
-      s[(idx >> logN) * NP + P::at(idx & (N - 1))] = zb[u];
+    for (int r = 0; r < 16; ++r) s[P::at(j * 16 + r)] = z[r];
+    __syncthreads();
+    Stages<C, FFT_EPT, false, LOGN, 16, LOGN - 4>::run(s, tw);
+  } else {
+#pragma unroll 1
+    for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
+      C zb[FFT_BATCH];
+#pragma unroll
+      for (int u = 0; u < FFT_BATCH; ++u) {
+        int idx = tid + (q0 + u) * NT;
+        int rb = idx >> logN, nn = idx & (N - 1);
+        int j = row0 + rb;
+        C z = mk<C>((T)0, (T)0);
+        if (j < h) {
+          size_t k = (size_t)j * w + 2 * nn;
+          z = *reinterpret_cast<const C*>(v + k);
+          if (WEIGHT) {
+            C ww = *reinterpret_cast<const C*>(wt + k);
+            z.x *= ww.x;
+            z.y *= ww.y;
+          }
+        }
+        zb[u] = z;
+      }
+#pragma unroll
+      for (int u = 0; u < FFT_BATCH; ++u) {
+        int idx = tid + (q0 + u) * NT;
+        s[(idx >> logN) * NP + P::at(idx & (N - 1))] = zb[u];
+      }
     }
+    __syncthreads();
+    smem_fft<C, FFT_EPT, false, LOGN>(s, tw);
   }
-  __syncthreads();
-  smem_fft<C, FFT_EPT, false, LOGN>(s, tw);
   // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
   constexpr int half_n = N / 2 + 1;
 #pragma unroll 2
@@ -977,18 +1002,13 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
     }
   }
   __syncthreads();
-  smem_fft<C, FFT_EPT, true, LOGN>(s, tw);
   const T inv_n = (T)1 / (T)N;
   Acc<2> acc;
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
-#pragma unroll 4
-  for (int idx = tid; idx < RB * N; idx += blockDim.x) {
-    int rb = idx >> logN, nn = idx & (N - 1);
-    int j = row0 + rb;
-    if (j >= h) continue;
+  // z = x[2 nn] + i x[2 nn + 1] of row j, scaled: the mode's output
+  auto emit = [&](int j, int nn, C z) {
     size_t k = (size_t)j * w + 2 * nn;
-    C z = cscale(s[rb * NP + P::at(nn)], inv_n);
     C* o = reinterpret_cast<C*>(out + k);
     if (MODE == INV_STORE) {
       *o = z;
@@ -1004,6 +1024,41 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       C rr = *reinterpret_cast<const C*>(r + k);
       acc.v[0] += (double)rr.x * (double)z.x + (double)rr.y * (double)z.y;
       acc.v[1] = fmax(acc.v[1], fmax(fabs((double)z.x), fabs((double)z.y)));
+    }
+  };
+  if constexpr (RB == 1 && LOGN >= 4) {
+    // one row per block: all stages but the last through shared memory; the last (radix RL,
+    // span N / RL, twiddles w^(r j)) hands each output to the mode's epilogue
+    constexpr int RL = last_radix(LOGN);
+    constexpr int LOGRL = RL == 16 ? 4 : RL == 8 ? 3 : RL == 4 ? 2 : 1;
+    constexpr int NSL = N / RL;
+    Stages<C, FFT_EPT, true, LOGN, 1, LOGN - LOGRL>::run(s, tw);
+#pragma unroll
+    for (int q = 0; q < FFT_EPT / RL; ++q) {
+      const int j = tid + q * NT;
+      C z[RL];
+#pragma unroll
+      for (int rr = 0; rr < RL; ++rr) z[rr] = s[P::at(j + rr * NSL)];
+      if (NSL > 1) {
+        C wv[RL];
+        stage_twiddles<C, RL, true>(tw, j, wv);
+#pragma unroll
+        for (int rr = 1; rr < RL; ++rr) z[rr] = cmul(z[rr], wv[rr]);
+      }
+      dft_r<C, RL, true>(z);
+      if (row0 < h) {
+#pragma unroll
+        for (int rr = 0; rr < RL; ++rr) emit(row0, j + rr * NSL, cscale(z[rr], inv_n));
+      }
+    }
+  } else {
+    smem_fft<C, FFT_EPT, true, LOGN>(s, tw);
+#pragma unroll 4
+    for (int idx = tid; idx < RB * N; idx += blockDim.x) {
+      int rb = idx >> logN, nn = idx & (N - 1);
+      int j = row0 + rb;
+      if (j >= h) continue;
+      emit(j, nn, cscale(s[rb * NP + P::at(nn)], inv_n));
     }
   }
   if (MODE == INV_STORE_DOT) {
