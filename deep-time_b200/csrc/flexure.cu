@@ -32,6 +32,7 @@
 #include <utility>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -80,6 +81,7 @@ struct Scalars {
   double rr_true, bb_true;  // ||b - A x||^2 and ||b||^2 in FP64, unscaled
   int replacements;         // residual replacements so far
   unsigned long long cond_if;  // the loop body's IF node around the replacement, 0 without one
+  int fault;                // a kernel's bounded wait ran out (the solve reports a device error)
 };
 
 __device__ __forceinline__ void set_cond(Scalars* S, unsigned int v) {
@@ -415,6 +417,11 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
     }
   }
 }
+
+}  // namespace dt
+#include "stencil_tma.cuh"
+#include <cudaTypedefs.h>
+namespace dt {
 
 // ---------------------------------------------------------------------------------------------
 // CG vector kernels (grid-stride).
@@ -1085,6 +1092,7 @@ __global__ void k_disarm(Scalars* S) {
 
 // A fresh solve state (keeps the problem fields, the bank and the handle slot cleared).
 __global__ void k_reset(Scalars* S) {
+  S->fault = 0;
   S->it = 0;
   S->stop = 0;
   S->started = 0;
@@ -1226,6 +1234,15 @@ struct dt_flex {
   std::vector<void*> allocs;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
+  // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
+  // and box shape, made on first use
+  bool tma = false;
+  struct MapEntry {
+    const void* p;
+    int elem, bw, bh;
+    CUtensorMap m;
+  };
+  std::vector<MapEntry> maps;
 };
 
 namespace dt {
@@ -1302,9 +1319,103 @@ static void free_graphs(Lane<T>& L) {
 
 static unsigned int ew_grid(const dt_flex* s) { return std::max(1u, std::min<unsigned int>(ceil_div(s->n, 256), (unsigned)s->sms * 8)); }
 
+// ---- the TMA stencil's host side ----
+static PFN_cuTensorMapEncodeTiled encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (PFN_cuTensorMapEncodeTiled) nullptr;
+    return (PFN_cuTensorMapEncodeTiled)p;
+  }();
+  return fn;
+}
+
+// The 2-D map of a w x h buffer with the given box (columns x rows), zero fill outside; cached.
+static bool tensor_map(dt_flex* s, const void* p, int elem, int bw, int bh, CUtensorMap* out) {
+  for (auto& e : s->maps)
+    if (e.p == p && e.elem == elem && e.bw == bw && e.bh == bh) {
+      *out = e.m;
+      return true;
+    }
+  PFN_cuTensorMapEncodeTiled fn = encode_tiled();
+  if (!fn || !p || ((size_t)p & 15)) return false;
+  dt_flex::MapEntry e{p, elem, bw, bh, {}};
+  cuuint64_t dims[2] = {(cuuint64_t)s->w, (cuuint64_t)s->h};
+  cuuint64_t strides[1] = {(cuuint64_t)s->w * (cuuint64_t)elem};
+  cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  cuuint32_t es[2] = {1, 1};
+  CUresult r = fn(&e.m, elem == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(p),
+                  dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return false;
+  s->maps.push_back(e);
+  *out = e.m;
+  return true;
+}
+
+// Resident blocks per SM of each TMA stencil instantiation ([double][mode]), set at create.
+static int g_tma_per_sm[2][7];
+
+template <class T, int MODE>
+static void tma_setup() {
+  using ST = TmaStage<T, MODE>;
+  cudaFuncSetAttribute(k_apply_tma<T, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, ST::SMEM);
+  int nb = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_apply_tma<T, MODE>, TBX * TTY, ST::SMEM);
+  g_tma_per_sm[sizeof(T) == 8][MODE] = std::max(nb, 1);
+}
+template <class T>
+static void tma_setup_all() {
+  tma_setup<T, AP_DOT>();
+  tma_setup<T, RESID>();
+  tma_setup<T, JAC_LEFT>();
+  tma_setup<T, JAC_FINAL>();
+  tma_setup<T, PLAIN>();
+  tma_setup<T, BEND>();
+  tma_setup<T, RESID_GATED>();
+}
+
+// The persistent TMA stencil; false (nothing launched) when a buffer cannot be mapped.
+template <class T, int MODE>
+static bool launch_apply_tma(dt_flex* s, const T* vsrc, const T* J, const T* part, const T* d, const T* c, const T* rb, T* y,
+                             Scalars* S, cudaStream_t st) {
+  using ST = TmaStage<T, MODE>;
+  CUtensorMap mv, mJ, mP, md, mc, mb;
+  if (!tensor_map(s, vsrc, sizeof(T), ST::P, ST::UR, &mv)) return false;
+  mJ = mP = mc = mb = mv;
+  if (ST::JAC && !tensor_map(s, J, sizeof(T), ST::P, ST::UR, &mJ)) return false;
+  if (MODE == JAC_FINAL && !tensor_map(s, part, sizeof(T), ST::P, ST::UR, &mP)) return false;
+  if (!tensor_map(s, d, sizeof(T), ST::P, ST::MR, &md)) return false;
+  if (ST::HAS_C && !tensor_map(s, c, sizeof(T), TBX, ST::TBY, &mc)) return false;
+  if (ST::HAS_B && !tensor_map(s, rb, sizeof(T), TBX, ST::TBY, &mb)) return false;
+  const int tiles_x = s->w / TBX, ntiles = tiles_x * (int)ceil_div(s->h, ST::TBY);
+  const int grid = std::max(1, std::min(ntiles, g_tma_per_sm[sizeof(T) == 8][MODE] * s->sms));
+  T inv = (T)(1.0 / (s->dx * s->dx));
+  k_apply_tma<T, MODE><<<grid, dim3(TBX, TTY), ST::SMEM, st>>>(mv, mJ, mP, md, mc, mb, s->w, s->h, inv, vsrc, J, part, d, y,
+                                                              s->partials, S, tiles_x, ntiles);
+  counted();
+  return true;
+}
+
 template <class T>
 static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* part, const T* d, const T* c, const T* rb, T* y,
                          Scalars* S, cudaStream_t st) {
+  if (s->tma) {
+    const T* vsrc = (mode == JAC_LEFT || mode == JAC_FINAL) ? rb : v;
+    bool done = false;
+    switch (mode) {
+      case AP_DOT: done = launch_apply_tma<T, AP_DOT>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case RESID: done = launch_apply_tma<T, RESID>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case JAC_LEFT: done = launch_apply_tma<T, JAC_LEFT>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case JAC_FINAL: done = launch_apply_tma<T, JAC_FINAL>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case PLAIN: done = launch_apply_tma<T, PLAIN>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case BEND: done = launch_apply_tma<T, BEND>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+      case RESID_GATED: done = launch_apply_tma<T, RESID_GATED>(s, vsrc, J, part, d, c, rb, y, S, st); break;
+    }
+    if (done) return;
+  }
   dim3 grid(ceil_div(s->w, TBX), ceil_div(s->h, tile_rows<T>())), block(TBX, TTY);
   T inv = (T)(1.0 / (s->dx * s->dx));
   switch (mode) {
@@ -1588,6 +1699,7 @@ struct HostProblem {
   int n;
 };
 __global__ void k_put_problem(Scalars* S, HostProblem p) {
+  S->fault = 0;
   S->tol = p.tol;
   S->max_it = p.max_it;
   S->rule = p.rule;
@@ -1750,6 +1862,10 @@ static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_r
   DT_TRY(run_pcg<double>(s, L, levels, p->host_loop));
   Scalars h;
   DT_TRY(read_scalars(s, L.S, &h));
+  if (h.fault) {
+    set_error("flexure solve: a kernel's wait for its tile copies ran out");
+    return DT_DEVICE_ERROR;
+  }
   count_loop(L, levels, p->host_loop, h.body_runs);
   int iterations = h.it;
   int stop = h.stop;
@@ -1816,6 +1932,10 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
     k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale); counted();
     resid64(s);
     DT_TRY(read_scalars(s, F.S, &hf));
+    if (hf.fault) {
+      set_error("flexure solve: a kernel's wait for its tile copies ran out");
+      return DT_DEVICE_ERROR;
+    }
     count_loop(F, levels, p->host_loop, hf.body_runs);
     iterations += hf.it;
     ++refinements;
@@ -1872,6 +1992,10 @@ static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool 
   resid64(s);
   Scalars h, hf;
   DT_TRY(read_scalars(s, F.S, &hf));
+  if (hf.fault) {
+    set_error("flexure solve: a kernel's wait for its tile copies ran out");
+    return DT_DEVICE_ERROR;
+  }
   count_loop(F, levels, p->host_loop, hf.body_runs, true);
   if (!p->host_loop) g_launches += 3LL * hf.replacements;  // the IF node's kernels, when they ran
   DT_TRY(read_scalars(s, L.S, &h));
@@ -1992,6 +2116,15 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   if ((st = dalloc(s, &s->rzpair, 2)) != DT_OK) return fail(st);
   transform_smem_attributes<double>();
   transform_smem_attributes<float>();
+  {
+    // the TMA stencil takes rasters whose rows are whole tiles; DT_STENCIL_TMA=0 turns it off
+    const char* env = getenv("DT_STENCIL_TMA");
+    s->tma = w % TBX == 0 && encode_tiled() != nullptr && !(env && env[0] == '0');
+    if (s->tma) {
+      tma_setup_all<double>();
+      tma_setup_all<float>();
+    }
+  }
   if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
     set_error("dt_flex_create: cudaEventCreate failed");
     return fail(DT_DEVICE_ERROR);
@@ -2228,7 +2361,12 @@ static dt_status apply_host(dt_flex* s, int mode, const double* d, const double*
   launch_apply<double>(s, mode, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, s->stream);
   DT_CUDA(cudaGetLastError());
   DT_CUDA(cudaMemcpyAsync(y, L.ap, bytes, cudaMemcpyDeviceToHost, s->stream));
-  DT_CUDA(cudaStreamSynchronize(s->stream));
+  Scalars hs;
+  DT_TRY(read_scalars(s, L.S, &hs));
+  if (hs.fault) {
+    set_error("flexure operator: a kernel's wait for its tile copies ran out");
+    return DT_DEVICE_ERROR;
+  }
   return DT_OK;
 }
 
