@@ -50,7 +50,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity) {
   }
   return false;
 }
-// A 2-D tile copy global -> shared (no multicast), completing on the mbarrier.
+// A 2-D tile copy from global memory into this CTA's shared memory, completing on the mbarrier.
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t mbar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
