@@ -21,6 +21,8 @@
 
 #include "common.cuh"
 #include "conv.cuh"
+#include "conv_tc.cuh"
+#include <cstdlib>
 
 namespace dt {
 
@@ -54,32 +56,57 @@ __global__ void k_pack_input(size_t npix, const float* __restrict__ x, bf16* __r
 }
 
 // 2 x 2 average pooling: out[n][y][x][c] = mean of in[n][2y..][2x..][c]
+// Eight channels (16 bytes) at a time: every channel count, stride and offset here is a
+// multiple of 8, and pixel counts fit 32 bits.
+__device__ __forceinline__ void bf8_to_f(uint4 v, float* f) {
+  const __nv_bfloat162* b = reinterpret_cast<const __nv_bfloat162*>(&v);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    float2 t = __bfloat1622float2(b[e]);
+    f[2 * e] = t.x;
+    f[2 * e + 1] = t.y;
+  }
+}
+__device__ __forceinline__ uint4 f_to_bf8(const float* f) {
+  uint4 v;
+  __nv_bfloat162* b = reinterpret_cast<__nv_bfloat162*>(&v);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) b[e] = __floats2bfloat162_rn(f[2 * e], f[2 * e + 1]);
+  return v;
+}
+
 __global__ void k_pool(int nimg, int h, int w, Tensor4 in, Tensor4 out) {
-  int ho = h / 2, wo = w / 2;
-  size_t total = (size_t)nimg * ho * wo * in.c;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
-    int c = (int)(k % in.c);
-    size_t p = k / in.c;
-    int x = (int)(p % wo), y = (int)((p / wo) % ho);
-    size_t n = p / ((size_t)wo * ho);
-    float s = 0.f;
+  const int ho = h / 2, wo = w / 2, c8 = in.c / 8;
+  const unsigned total = (unsigned)nimg * ho * wo * c8;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    unsigned c = k % c8, p = k / c8;
+    unsigned x = p % wo, r = p / wo, y = r % ho, n = r / ho;
+    float s[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
     for (int dy = 0; dy < 2; ++dy)
-      for (int dx = 0; dx < 2; ++dx)
-        s += __bfloat162float(in.p[(((n * h) + 2 * y + dy) * w + 2 * x + dx) * in.stride + in.off + c]);
-    out.p[p * out.stride + out.off + c] = __float2bfloat16(0.25f * s);
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx) {
+        size_t q = ((size_t)(n * h + 2 * y + dy) * w + 2 * x + dx) * in.stride + in.off + c * 8;
+        float f[8];
+        bf8_to_f(*reinterpret_cast<const uint4*>(in.p + q), f);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s[e] += f[e];
+      }
+#pragma unroll
+    for (int e = 0; e < 8; ++e) s[e] *= 0.25f;
+    *reinterpret_cast<uint4*>(out.p + (size_t)p * out.stride + out.off + c * 8) = f_to_bf8(s);
   }
 }
 
 // nearest-neighbour upsampling into a slice: out[n][y][x][c] = in[n][y/2][x/2][c]
 __global__ void k_upsample(int nimg, int h, int w, Tensor4 in, Tensor4 out) {
-  size_t total = (size_t)nimg * h * w * in.c;
-  int hi = h / 2, wi = w / 2;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < total; k += (size_t)gridDim.x * blockDim.x) {
-    int c = (int)(k % in.c);
-    size_t p = k / in.c;
-    int x = (int)(p % w), y = (int)((p / w) % h);
-    size_t n = p / ((size_t)w * h);
-    out.p[p * out.stride + out.off + c] = in.p[(((n * hi) + y / 2) * wi + x / 2) * in.stride + in.off + c];
+  const int hi = h / 2, wi = w / 2, c8 = in.c / 8;
+  const unsigned total = (unsigned)nimg * h * w * c8;
+  for (unsigned k = blockIdx.x * blockDim.x + threadIdx.x; k < total; k += gridDim.x * blockDim.x) {
+    unsigned c = k % c8, p = k / c8;
+    unsigned x = p % w, r = p / w, y = r % h, n = r / h;
+    size_t src = ((size_t)(n * hi + y / 2) * wi + x / 2) * in.stride + in.off + c * 8;
+    *reinterpret_cast<uint4*>(out.p + (size_t)p * out.stride + out.off + c * 8) = *reinterpret_cast<const uint4*>(in.p + src);
   }
 }
 
@@ -126,7 +153,12 @@ __global__ void k_head_fwd(size_t npix, Tensor4 act, const float* __restrict__ W
   for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
     float s = bh[0];
     const bf16* a = act.p + p * act.stride + act.off;
-    for (int c = 0; c < act.c; ++c) s += Wh[c] * __bfloat162float(a[c]);
+    for (int c = 0; c < act.c; c += 8) {
+      float f[8];
+      bf8_to_f(*reinterpret_cast<const uint4*>(a + c), f);
+#pragma unroll
+      for (int e = 0; e < 8; ++e) s += Wh[c + e] * f[e];
+    }
     pred[p] = s;
   }
 }
@@ -246,6 +278,11 @@ struct dt_unet {
   cudaStream_t stream = nullptr;
   bool own_stream = true;  // false once bound to a caller's stream (dt_unet_set_stream)
   int sms = 148;
+  // forward and input-gradient convolutions on tcgen05 when DT_UNET_TC=1 (default: the mma.sync
+  // kernels, faster at this network's channel counts); a device flag the tcgen05 kernels' bounded
+  // waits set when one runs out
+  bool tc = false;
+  int* tc_fault = nullptr;
 };
 
 namespace dt {
@@ -312,7 +349,59 @@ static dt_status unet_batch(dt_unet* u, int B, int H, int W) {
 
 static Tensor4 T4(bf16* p, int stride, int off, int c) { return Tensor4{p, stride, off, c}; }
 
+// Dynamic shared memory of every tcgen05 convolution instantiation (more than the default 48 KB).
+template <int EPI>
+static dt_status conv_tc_attributes_epi() {
+  DT_CUDA(cudaFuncSetAttribute(k_conv3x3_tc<32, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<32>()));
+  DT_CUDA(cudaFuncSetAttribute(k_conv3x3_tc<64, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<64>()));
+  DT_CUDA(cudaFuncSetAttribute(k_conv3x3_tc<128, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<128>()));
+  DT_CUDA(cudaFuncSetAttribute(k_conv3x3_tc<256, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<256>()));
+  return DT_OK;
+}
+static dt_status conv_tc_attributes() {
+  DT_TRY(conv_tc_attributes_epi<EPI_BIAS_RELU>());
+  DT_TRY(conv_tc_attributes_epi<EPI_BIAS>());
+  DT_TRY(conv_tc_attributes_epi<EPI_MASK>());
+  DT_TRY(conv_tc_attributes_epi<EPI_STORE>());
+  return DT_OK;
+}
+
+// The tcgen05 convolution for a problem of `n` output channels over B h w pixels, with B source
+// `Bk` (K-major after mirroring the taps); false when the shape does not suit it.
+template <int EPI>
+static bool conv_tc(dt_unet* u, int B, int h, int w, Tensor4 in, const bf16* Bk, int n, const float* bias, Tensor4 out,
+                    Tensor4 mask, cudaStream_t st) {
+  size_t pixels = (size_t)B * h * w;
+  if (!u->tc || pixels % 128 != 0 || in.c % 32 != 0 || n % 32 != 0 || pixels / 128 > 0x7fffffff) return false;
+#ifndef DT_TC_MAX_N
+#define DT_TC_MAX_N 128
+#endif
+  int bn = (n % 256 == 0 && DT_TC_MAX_N >= 256) ? 256 : (n % 128 == 0 && DT_TC_MAX_N >= 128) ? 128 : n % 64 == 0 ? 64 : 32;
+  dim3 grid((unsigned)(pixels / 128), n / bn);
+  auto go = [&](auto kernel, int smem) {
+    kernel<<<grid, 128, smem, st>>>(B, h, w, in, Bk, n, bias, out, mask, u->tc_fault);
+  };
+  if (bn == 256)
+    go(k_conv3x3_tc<256, EPI>, tc_smem_bytes<256>());
+  else if (bn == 128)
+    go(k_conv3x3_tc<128, EPI>, tc_smem_bytes<128>());
+  else if (bn == 64)
+    go(k_conv3x3_tc<64, EPI>, tc_smem_bytes<64>());
+  else
+    go(k_conv3x3_tc<32, EPI>, tc_smem_bytes<32>());
+  count_launch();
+  return true;
+}
+
 static void conv_fwd(dt_unet* u, const ConvLayer& L, int B, int h, int w, Tensor4 in, Tensor4 out, bool relu, cudaStream_t st) {
+  {
+    // B[tap][co][ci] = W[tap][ci][co] = WT[8 - tap][co][ci]
+    const float* bias = u->prm + L.b_off;
+    Tensor4 none = T4(nullptr, 0, 0, 0);
+    bool done = relu ? conv_tc<EPI_BIAS_RELU>(u, B, h, w, in, L.WT, L.cout, bias, out, none, st)
+                     : conv_tc<EPI_BIAS>(u, B, h, w, in, L.WT, L.cout, bias, out, none, st);
+    if (done) return;
+  }
   bool wide = L.cout % 64 == 0;
   dim3 grid((unsigned)((size_t)B * h * (w / 64)), L.cout / (wide ? 64 : 32));
   const float* bias = u->prm + L.b_off;
@@ -340,6 +429,12 @@ static void conv_dgrad(dt_unet* u, const ConvLayer& L, int B, int h, int w, Tens
   Tensor4 none = T4(nullptr, 0, 0, 0);
   Tensor4 gout = T4(gin.p, gin.stride, gin.off, cout);
   Tensor4 gg = T4(g.p, g.stride, g.off, L.cout);
+  {
+    // the transposed problem's B[tap][n = ci][k = co] = W[8 - tap][ci][co]
+    bool done = mask ? conv_tc<EPI_MASK>(u, B, h, w, gg, L.W, cout, nullptr, gout, *mask, st)
+                     : conv_tc<EPI_STORE>(u, B, h, w, gg, L.W, cout, nullptr, gout, none, st);
+    if (done) return;
+  }
   if (wide) {
     if (mask)
       k_conv3x3<64, EPI_MASK><<<grid, 128, 0, st>>>(B, h, w, gg, L.WT, nullptr, gout, *mask);
@@ -605,6 +700,20 @@ dt_status dt_unet_create(int base_channels, unsigned long long seed, dt_unet** o
     dt_unet_destroy(u);
     return st;
   }
+  {
+    const char* env = getenv("DT_UNET_TC");
+    u->tc = prop.major >= 10 && env && env[0] == '1';
+    if (u->tc && (st = dt::conv_tc_attributes()) != DT_OK) {
+      dt_unet_destroy(u);
+      return st;
+    }
+    st = dt::ualloc(u->allocs, reinterpret_cast<void**>(&u->tc_fault), sizeof(int));
+    if (st == DT_OK && cudaMemset(u->tc_fault, 0, sizeof(int)) != cudaSuccess) st = DT_DEVICE_ERROR;
+    if (st != DT_OK) {
+      dt_unet_destroy(u);
+      return st;
+    }
+  }
   *out = u;
   return DT_OK;
 }
@@ -639,7 +748,14 @@ dt_status dt_unet_set_stream(dt_unet* u, void* stream) {
 // x: [B][H][W][2] FP32 (device), y: [B][H][W] FP32 (device)
 dt_status dt_unet_predict_dev(dt_unet* u, const float* x, float* y, int B, int H, int W) {
   DT_TRY(dt::unet_predict_on(u, u ? u->stream : nullptr, x, y, B, H, W));
+  DT_CUDA(cudaGetLastError());
   DT_CUDA(cudaStreamSynchronize(u->stream));
+  int fault = 0;
+  DT_CUDA(cudaMemcpy(&fault, u->tc_fault, sizeof(int), cudaMemcpyDeviceToHost));
+  if (fault) {
+    set_error("dt_unet_predict_dev: a tensor-core convolution's wait ran out");
+    return DT_DEVICE_ERROR;
+  }
   return DT_OK;
 }
 

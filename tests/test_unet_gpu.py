@@ -142,3 +142,27 @@ def test_training_reduces_the_loss_and_weights_round_trip(tmp_path):
     model.predict_dev(x[0].data_ptr(), y1.data_ptr(), 1, H, W)
     other.predict_dev(x[0].data_ptr(), y2.data_ptr(), 1, H, W)
     assert torch.equal(y1, y2)
+
+
+def test_the_tensor_memory_path_reproduces_the_default_one(monkeypatch):
+    # the tcgen05 convolutions (DT_UNET_TC=1, read when a model is made) against the default
+    # mma.sync ones on the same weights: both sum exact BF16 products in FP32 in the same K order
+    rng = np.random.default_rng(3)
+    B, H, W = 2, 16, 512
+    x = torch.from_numpy(rng.standard_normal((B, H, W, 2)).astype(np.float32)).cuda()
+    t = torch.from_numpy(rng.standard_normal((B, H, W)).astype(np.float32) * 0.1).cuda()
+    monkeypatch.setenv("DT_UNET_TC", "1")
+    tc = U.UNet(seed=11)
+    monkeypatch.setenv("DT_UNET_TC", "0")
+    ref = U.UNet(seed=11)
+    y1 = torch.empty((B, H, W), device="cuda")
+    y2 = torch.empty((B, H, W), device="cuda")
+    tc.predict_dev(x.data_ptr(), y1.data_ptr(), B, H, W)
+    ref.predict_dev(x.data_ptr(), y2.data_ptr(), B, H, W)
+    assert torch.allclose(y1, y2, rtol=1e-3, atol=1e-3 * float(y2.abs().max())), float((y1 - y2).abs().max())
+    l1 = tc.loss_and_grad_dev(x.data_ptr(), t.data_ptr(), B, H, W)
+    g1 = tc.gradients()
+    l2 = ref.loss_and_grad_dev(x.data_ptr(), t.data_ptr(), B, H, W)
+    g2 = ref.gradients()
+    assert abs(l1 - l2) <= 1e-3 * abs(l2)
+    assert np.linalg.norm(g1 - g2) <= 1e-3 * np.linalg.norm(g2)
