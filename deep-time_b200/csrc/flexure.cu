@@ -2194,8 +2194,18 @@ __global__ void k_unet_normalise(size_t nc, float* __restrict__ x, const double*
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) x[2 * k] *= inv;
 }
 
-// The prediction back on the raster, in metres: bilinear from the coarse cells' centres with x
-// wrapping and rows clamping (prolong_linear, flexure.rs:1816-1844), times rms(b_coarse) / mean(c).
+// The prediction back on the raster, in metres: Catmull-Rom cubic interpolation from the coarse
+// cells' centres (x wrapping, rows clamping), times rms(b_coarse) / mean(c). The cubic is C1, so
+// the guess has no kinks along the coarse cells' edges; the operator weighs curvature, and a
+// bilinear prolongation (prolong_linear, flexure.rs:1816-1844) leaves kinks that cost the guess
+// much of its energy-norm accuracy.
+__device__ __forceinline__ void catmull_rom(double t, double* c) {
+  double t2 = t * t, t3 = t2 * t;
+  c[0] = 0.5 * (-t3 + 2.0 * t2 - t);
+  c[1] = 0.5 * (3.0 * t3 - 5.0 * t2 + 2.0);
+  c[2] = 0.5 * (-3.0 * t3 + 4.0 * t2 + t);
+  c[3] = 0.5 * (t3 - t2);
+}
 __global__ void k_unet_prolong(int w, int h, int f, const float* __restrict__ y, double* __restrict__ x, const double* sums) {
   int ws = w / f, hs = h / f;
   size_t n = (size_t)w * h;
@@ -2205,11 +2215,22 @@ __global__ void k_unet_prolong(int w, int h, int f, const float* __restrict__ y,
     double xf = (i + 0.5) / f - 0.5;
     double yf = fmin(fmax((j + 0.5) / f - 0.5, 0.0), (double)(hs - 1));
     double x0 = floor(xf), y0 = floor(yf);
-    double tx = xf - x0, ty = yf - y0;
-    int i0 = (((int)x0 % ws) + ws) % ws, i1 = (i0 + 1) % ws;
-    int j0 = (int)y0, j1 = min(j0 + 1, hs - 1);
-    double v = ((double)y[(size_t)j0 * ws + i0] * (1.0 - tx) + (double)y[(size_t)j0 * ws + i1] * tx) * (1.0 - ty) +
-               ((double)y[(size_t)j1 * ws + i0] * (1.0 - tx) + (double)y[(size_t)j1 * ws + i1] * tx) * ty;
+    double cx[4], cy[4];
+    catmull_rom(xf - x0, cx);
+    catmull_rom(yf - y0, cy);
+    int ix = (int)x0, iy = (int)y0;
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      int jj = min(max(iy - 1 + b, 0), hs - 1);
+      double row = 0.0;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        int ii = ((ix - 1 + a) % ws + ws) % ws;
+        row += cx[a] * (double)y[(size_t)jj * ws + ii];
+      }
+      v += cy[b] * row;
+    }
     x[k] = v * scale;
   }
 }

@@ -182,8 +182,9 @@ dt_status dt_unet_save(dt_unet* u, const char* path);
 dt_status dt_unet_load(dt_unet* u, const char* path);
 /* Attach a model to a flexure handle for DT_WARM_UNET: its first guess is predicted on the model's
  * cells (model_dx metres, a power-of-two multiple of the raster's dx; block means of b and
- * log10 D), prolonged bilinearly (prolong_linear, flexure.rs:1816-1844), and kept only when
- * r0.M^-1 r0 < b.M^-1 b. NULL detaches. */
+ * log10 D), prolonged by Catmull-Rom cubic interpolation (C1, unlike the reference's bilinear
+ * prolong_linear, flexure.rs:1816-1844, whose kinks the operator's curvature energy penalises),
+ * and kept only when r0.M^-1 r0 < b.M^-1 b. NULL detaches. */
 dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
 
 /* Benchmark support: the average device time (ms) of each hot kernel of one PCG iteration,
