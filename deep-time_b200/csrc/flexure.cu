@@ -1201,6 +1201,9 @@ struct Lane {
   T *d = nullptr, *c = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
   T *J = nullptr, *wt[3] = {nullptr, nullptr, nullptr}, *left = nullptr, *part = nullptr;
   cplx<T>* half = nullptr;
+  // the bank's levels 1 and 2 run beside level 0 (their own spectra and outputs)
+  cplx<T>* half_side[2] = {nullptr, nullptr};
+  T* part_side[2] = {nullptr, nullptr};
   Tables<T> tab;
   Scalars* S = nullptr;
   cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
@@ -1237,6 +1240,9 @@ struct dt_flex {
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
   // and box shape, made on first use
   bool tma = false;
+  // the bank levels' side streams and their fork / join events
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
   struct MapEntry {
     const void* p;
     int elem, bw, bh;
@@ -1301,6 +1307,10 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   for (T** p : {&L.d, &L.c, &L.x, &L.r, &L.z, &L.p, &L.ap, &L.J, &L.wt[0], &L.wt[1], &L.wt[2], &L.left, &L.part})
     DT_TRY(dalloc(s, p, n));
   DT_TRY(dalloc(s, &L.half, (size_t)s->h * s->N));
+  for (int k = 0; k < 2; ++k) {
+    DT_TRY(dalloc(s, &L.half_side[k], (size_t)s->h * s->N));
+    DT_TRY(dalloc(s, &L.part_side[k], n));
+  }
   DT_TRY(make_tables(s, L.tab));
   DT_TRY(dalloc(s, &L.S, 1));
   DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
@@ -1501,38 +1511,59 @@ static void transform_smem_attributes() {
 }
 
 template <class T>
-static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, const FftGeo& g, Scalars* S, cudaStream_t st) {
+static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cplx<T>* half, const FftGeo& g, Scalars* S,
+                            cudaStream_t st) {
   int logn = ilog2(s->N);
   if (wt)
-    rows_fwd_fn<T, true>(logn, LogSeq{})<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row,
+    rows_fwd_fn<T, true>(logn, LogSeq{})<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, in, wt, half, L.tab.tw_row,
                                                                                   L.tab.post, S);
   else
-    rows_fwd_fn<T, false>(logn, LogSeq{})<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, in, wt, L.half, L.tab.tw_row,
+    rows_fwd_fn<T, false>(logn, LogSeq{})<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, in, wt, half, L.tab.tw_row,
                                                                                    L.tab.post, S);
   counted();
 }
 template <class T>
-static void launch_cols(dt_flex* s, Lane<T>& L, const FftGeo& g, int level, Scalars* S, cudaStream_t st) {
-  cols_fn<T>(ilog2(s->h), LogSeq{})<<<g.cgrid, g.cthreads, g.csmem, st>>>(s->N, L.half, L.tab.tw_col, L.tab.omega, L.tab.lx,
+static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, int level, Scalars* S, cudaStream_t st) {
+  cols_fn<T>(ilog2(s->h), LogSeq{})<<<g.cgrid, g.cthreads, g.csmem, st>>>(s->N, half, L.tab.tw_col, L.tab.omega, L.tab.lx,
                                                                           L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S, level);
   counted();
 }
 template <class T>
-static void launch_rows_inv(dt_flex* s, Lane<T>& L, int mode, T* out, const T* wt, const T* r, const FftGeo& g, Scalars* S,
-                            cudaStream_t st) {
-  rows_inv_for<T>(mode, ilog2(s->N))<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, L.half, out, wt, r, L.tab.tw_row,
+static void launch_rows_inv(dt_flex* s, Lane<T>& L, int mode, const cplx<T>* half, T* out, const T* wt, const T* r,
+                            const FftGeo& g, Scalars* S, cudaStream_t st) {
+  rows_inv_for<T>(mode, ilog2(s->N))<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, half, out, wt, r, L.tab.tw_row,
                                                                            L.tab.post, s->partials, S);
   counted();
 }
 
-// One spectral solve of one bank level: out (op)= S_k (in * wt) (* wt).
+// One spectral solve of one bank level: out (op)= S_k (in * wt) (* wt), through the spectrum
+// buffer `half` (the lane's own when null).
 template <class T>
 static void launch_spectral(dt_flex* s, Lane<T>& L, const T* in, const T* wt, T* out, int inv_mode, int level, Scalars* S,
-                            cudaStream_t st) {
+                            cudaStream_t st, cplx<T>* half = nullptr) {
   FftGeo g = fft_geometry<T>(s);
-  launch_rows_fwd<T>(s, L, in, wt, g, S, st);
-  launch_cols<T>(s, L, g, level, S, st);
-  launch_rows_inv<T>(s, L, inv_mode, out, wt, inv_mode == INV_STORE_DOT ? in : nullptr, g, S, st);
+  if (!half) half = L.half;
+  launch_rows_fwd<T>(s, L, in, wt, half, g, S, st);
+  launch_cols<T>(s, L, half, g, level, S, st);
+  launch_rows_inv<T>(s, L, inv_mode, half, out, wt, inv_mode == INV_STORE_DOT ? in : nullptr, g, S, st);
+}
+
+// part = part + p1 + p2 (16-byte words; the buffers are the lane's own)
+template <class T>
+__global__ void __launch_bounds__(256) k_sum3(size_t n, T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ c) {
+  constexpr int V = 16 / sizeof(T);
+  using W = Vec16<T>;
+  const size_t nv = n / V, stride = (size_t)gridDim.x * blockDim.x, t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  W* av = reinterpret_cast<W*>(a);
+  const W* bv = reinterpret_cast<const W*>(b);
+  const W* cv = reinterpret_cast<const W*>(c);
+  for (size_t k = t0; k < nv; k += stride) {
+    W x = av[k], y = bv[k], z = cv[k];
+#pragma unroll
+    for (int e = 0; e < V; ++e) x.a[e] = (x.a[e] + y.a[e]) + z.a[e];
+    av[k] = x;
+  }
+  for (size_t k = nv * V + t0; k < n; k += stride) a[k] = (a[k] + b[k]) + c[k];
 }
 
 // z = M^-1 r with r.z and max|z| reduced into S (finish_precond). levels 1: one spectral solve at
@@ -1544,8 +1575,21 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
     return;
   }
   launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, r, L.left, L.S, st);  // left = r - A(J r)
-  for (int k = 0; k < 3; ++k)  // part = sum_k w_k S_k(w_k left)
-    launch_spectral<T>(s, L, L.left, L.wt[k], L.part, k == 0 ? INV_STORE_W : INV_ACCUM, k, L.S, st);
+  // part = sum_k w_k S_k(w_k left): the three levels' transforms are independent, so levels 1 and
+  // 2 run on side streams (parallel branches when captured into the loop graph) into their own
+  // buffers, summed before the final pass
+  cudaEventRecord(s->ev_fork, st);
+  cudaStreamWaitEvent(s->side[0], s->ev_fork, 0);
+  cudaStreamWaitEvent(s->side[1], s->ev_fork, 0);
+  launch_spectral<T>(s, L, L.left, L.wt[0], L.part, INV_STORE_W, 0, L.S, st);
+  launch_spectral<T>(s, L, L.left, L.wt[1], L.part_side[0], INV_STORE_W, 1, L.S, s->side[0], L.half_side[0]);
+  launch_spectral<T>(s, L, L.left, L.wt[2], L.part_side[1], INV_STORE_W, 2, L.S, s->side[1], L.half_side[1]);
+  cudaEventRecord(s->ev_join[0], s->side[0]);
+  cudaEventRecord(s->ev_join[1], s->side[1]);
+  cudaStreamWaitEvent(st, s->ev_join[0], 0);
+  cudaStreamWaitEvent(st, s->ev_join[1], 0);
+  k_sum3<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.part, L.part_side[0], L.part_side[1]);
+  counted();
   launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, r, z, L.S, st);  // z = u + J(r - A u)
 }
 
@@ -2059,6 +2103,11 @@ dt_status dt_flex_destroy(dt_flex* s) {
   for (void* p : s->allocs) cudaFree(p);
   if (s->ev0) cudaEventDestroy(s->ev0);
   if (s->ev1) cudaEventDestroy(s->ev1);
+  for (int k = 0; k < 2; ++k) {
+    if (s->side[k]) cudaStreamDestroy(s->side[k]);
+    if (s->ev_join[k]) cudaEventDestroy(s->ev_join[k]);
+  }
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
   return DT_OK;
@@ -2124,6 +2173,16 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
       tma_setup_all<double>();
       tma_setup_all<float>();
     }
+  }
+  for (int k = 0; k < 2; ++k)
+    if (cudaStreamCreateWithFlags(&s->side[k], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->ev_join[k], cudaEventDisableTiming) != cudaSuccess) {
+      set_error("dt_flex_create: side streams");
+      return fail(DT_DEVICE_ERROR);
+    }
+  if (cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess) {
+    set_error("dt_flex_create: events");
+    return fail(DT_DEVICE_ERROR);
   }
   if (cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
     set_error("dt_flex_create: cudaEventCreate failed");
@@ -2487,13 +2546,13 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
         case 0: launch_apply<T>(s, AP_DOT, L.p, nullptr, nullptr, L.d, L.c, nullptr, L.ap, L.S, st); break;
         case 1: k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); break;
         case 2: k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); break;
-        case 3: launch_rows_fwd<T>(s, L, L.r, nullptr, g, L.S, st); break;
-        case 4: launch_cols<T>(s, L, g, 0, L.S, st); break;
-        case 5: launch_rows_inv<T>(s, L, INV_STORE_DOT, L.z, nullptr, L.r, g, L.S, st); break;
+        case 3: launch_rows_fwd<T>(s, L, L.r, nullptr, L.half, g, L.S, st); break;
+        case 4: launch_cols<T>(s, L, L.half, g, 0, L.S, st); break;
+        case 5: launch_rows_inv<T>(s, L, INV_STORE_DOT, L.half, L.z, nullptr, L.r, g, L.S, st); break;
         case 6: launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, L.r, L.left, L.S, st); break;
         case 7: launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, L.r, L.z, L.S, st); break;
-        case 8: launch_rows_fwd<T>(s, L, L.left, L.wt[0], g, L.S, st); break;
-        case 9: launch_rows_inv<T>(s, L, INV_ACCUM, L.part, L.wt[0], nullptr, g, L.S, st); break;
+        case 8: launch_rows_fwd<T>(s, L, L.left, L.wt[0], L.half, g, L.S, st); break;
+        case 9: launch_rows_inv<T>(s, L, INV_ACCUM, L.half, L.part, L.wt[0], nullptr, g, L.S, st); break;
       }
     };
     one();  // warm
