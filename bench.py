@@ -41,7 +41,7 @@ import numpy as np  # noqa: E402
 W, H, DX, SIGMA = 4096, 2048, 2500.0, 32.0
 TOL = 1e-8
 KERNEL_NAMES = ["flex_apply", "cg_update", "cg_direction", "fft_rows_fwd", "dct_cols_divide_idct", "fft_rows_inv_dot",
-                "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_accumulate"]
+                "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_bank"]
 WEIGHTS = os.path.join(ROOT, "deep-time_b200", "weights", "unet_flexure.bin")
 MODEL_DX = 10_000.0  # the U-Net's cell size: trained on 512 x 256 rasters of 10 km
 METRIC = "flexure solves/s to relative residual 1e-8 @4096x2048 (time-to-1e-8 per solve = 1000/value ms)"

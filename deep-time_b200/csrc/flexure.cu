@@ -658,7 +658,9 @@ __global__ void __launch_bounds__(256) k_bank_weights(int w, int h, const T* __r
 // by N = w/2 complex values. Each thread of a transform kernel holds FFT_EPT complex values per
 // FFT stage, so a block of `batch` sequences of length L has batch * L / FFT_EPT threads.
 
-enum { INV_STORE = 0, INV_ACCUM = 1, INV_STORE_DOT = 2, INV_STORE_W = 3 };
+// INV_BANK: the bank's three levels in one pass, out = sum_k wt_k x_k, the levels' spectra and
+// weights consecutive (half + k h N, wt + k w h)
+enum { INV_STORE = 0, INV_STORE_DOT = 2, INV_STORE_W = 3, INV_BANK = 4 };
 // Correctly rounded reciprocals (double: one division; float: the intrinsic).
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
@@ -964,6 +966,18 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   constexpr int half_n = N / 2 + 1;
   constexpr int NT = RB * N / FFT_EPT;  // the block's threads (fft_geometry)
   constexpr int IB = FFT_BATCH / 2;     // pairs (X[k], X[N-k]) loaded per batch
+  constexpr int LEVELS = MODE == INV_BANK ? 3 : 1;
+  const T inv_n = (T)1 / (T)N;
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  const cplx<T>* const half0 = half;
+  const T* const wt0 = wt;
+#pragma unroll 1
+  for (int lv = 0; lv < LEVELS; ++lv) {
+  half = half0 + (size_t)lv * h * N;
+  wt = wt0 + (size_t)lv * w * h;
+  if (lv > 0) __syncthreads();  // the previous level's last reads of s are done
 #pragma unroll 1
   for (int base = tid; base < RB * half_n; base += IB * NT) {
     C xkb[IB], xnb[IB];
@@ -1009,20 +1023,17 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
     }
   }
   __syncthreads();
-  const T inv_n = (T)1 / (T)N;
-  Acc<2> acc;
-  acc.v[0] = 0.0;
-  acc.v[1] = 0.0;
-  // z = x[2 nn] + i x[2 nn + 1] of row j, scaled: the mode's output
+  // z = x[2 nn] + i x[2 nn + 1] of row j, scaled: the mode's output (the bank's first level
+  // stores, the others add to what the same thread stored)
   auto emit = [&](int j, int nn, C z) {
     size_t k = (size_t)j * w + 2 * nn;
     C* o = reinterpret_cast<C*>(out + k);
     if (MODE == INV_STORE) {
       *o = z;
-    } else if (MODE == INV_STORE_W) {
+    } else if (MODE == INV_STORE_W || (MODE == INV_BANK && lv == 0)) {
       C ww = *reinterpret_cast<const C*>(wt + k);
       *o = mk<C>(z.x * ww.x, z.y * ww.y);
-    } else if (MODE == INV_ACCUM) {
+    } else if (MODE == INV_BANK) {
       C ww = *reinterpret_cast<const C*>(wt + k);
       C prev = *o;
       *o = mk<C>(prev.x + z.x * ww.x, prev.y + z.y * ww.y);
@@ -1068,6 +1079,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       emit(j, nn, cscale(s[rb * NP + P::at(nn)], inv_n));
     }
   }
+  }  // levels
   if (MODE == INV_STORE_DOT) {
     const int kind[2] = {0, 1};
     if (reduce_partials<2>(acc, kind, partials, &S->ticket[SITE_PRECOND], gridDim.x) && tid == 0) finish_precond(S, acc.v[0], acc.v[1]);
@@ -1201,9 +1213,9 @@ struct Lane {
   T *d = nullptr, *c = nullptr, *x = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *ap = nullptr;
   T *J = nullptr, *wt[3] = {nullptr, nullptr, nullptr}, *left = nullptr, *part = nullptr;
   cplx<T>* half = nullptr;
-  // the bank's levels 1 and 2 run beside level 0 (their own spectra and outputs)
+  // the bank's levels 1 and 2 transform beside level 0, into their own spectra: the three
+  // spectra are consecutive (half + k h N), as are the three weights (wt[k] = wt[0] + k n)
   cplx<T>* half_side[2] = {nullptr, nullptr};
-  T* part_side[2] = {nullptr, nullptr};
   Tables<T> tab;
   Scalars* S = nullptr;
   cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
@@ -1304,13 +1316,14 @@ static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
 template <class T>
 static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   size_t n = s->n;
-  for (T** p : {&L.d, &L.c, &L.x, &L.r, &L.z, &L.p, &L.ap, &L.J, &L.wt[0], &L.wt[1], &L.wt[2], &L.left, &L.part})
-    DT_TRY(dalloc(s, p, n));
-  DT_TRY(dalloc(s, &L.half, (size_t)s->h * s->N));
-  for (int k = 0; k < 2; ++k) {
-    DT_TRY(dalloc(s, &L.half_side[k], (size_t)s->h * s->N));
-    DT_TRY(dalloc(s, &L.part_side[k], n));
-  }
+  for (T** p : {&L.d, &L.c, &L.x, &L.r, &L.z, &L.p, &L.ap, &L.J, &L.left, &L.part}) DT_TRY(dalloc(s, p, n));
+  DT_TRY(dalloc(s, &L.wt[0], 3 * n));
+  L.wt[1] = L.wt[0] + n;
+  L.wt[2] = L.wt[0] + 2 * n;
+  const size_t hn = (size_t)s->h * s->N;
+  DT_TRY(dalloc(s, &L.half, 3 * hn));
+  L.half_side[0] = L.half + hn;
+  L.half_side[1] = L.half + 2 * hn;
   DT_TRY(make_tables(s, L.tab));
   DT_TRY(dalloc(s, &L.S, 1));
   DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
@@ -1492,7 +1505,7 @@ static RowsInvFn<T> rows_inv_for(int mode, int logn) {
   switch (mode) {
     case INV_STORE: return rows_inv_fn<T, INV_STORE>(logn, LogSeq{});
     case INV_STORE_W: return rows_inv_fn<T, INV_STORE_W>(logn, LogSeq{});
-    case INV_ACCUM: return rows_inv_fn<T, INV_ACCUM>(logn, LogSeq{});
+    case INV_BANK: return rows_inv_fn<T, INV_BANK>(logn, LogSeq{});
     default: return rows_inv_fn<T, INV_STORE_DOT>(logn, LogSeq{});
   }
 }
@@ -1505,7 +1518,7 @@ static void transform_smem_attributes() {
     cudaFuncSetAttribute(rows_fwd_fn<T, true>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(rows_fwd_fn<T, false>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(cols_fn<T>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    for (int m : {INV_STORE, INV_STORE_W, INV_ACCUM, INV_STORE_DOT})
+    for (int m : {INV_STORE, INV_STORE_W, INV_STORE_DOT, INV_BANK})
       cudaFuncSetAttribute(rows_inv_for<T>(m, l), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   }
 }
@@ -1548,24 +1561,6 @@ static void launch_spectral(dt_flex* s, Lane<T>& L, const T* in, const T* wt, T*
   launch_rows_inv<T>(s, L, inv_mode, half, out, wt, inv_mode == INV_STORE_DOT ? in : nullptr, g, S, st);
 }
 
-// part = part + p1 + p2 (16-byte words; the buffers are the lane's own)
-template <class T>
-__global__ void __launch_bounds__(256) k_sum3(size_t n, T* __restrict__ a, const T* __restrict__ b, const T* __restrict__ c) {
-  constexpr int V = 16 / sizeof(T);
-  using W = Vec16<T>;
-  const size_t nv = n / V, stride = (size_t)gridDim.x * blockDim.x, t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  W* av = reinterpret_cast<W*>(a);
-  const W* bv = reinterpret_cast<const W*>(b);
-  const W* cv = reinterpret_cast<const W*>(c);
-  for (size_t k = t0; k < nv; k += stride) {
-    W x = av[k], y = bv[k], z = cv[k];
-#pragma unroll
-    for (int e = 0; e < V; ++e) x.a[e] = (x.a[e] + y.a[e]) + z.a[e];
-    av[k] = x;
-  }
-  for (size_t k = nv * V + t0; k < n; k += stride) a[k] = (a[k] + b[k]) + c[k];
-}
-
 // z = M^-1 r with r.z and max|z| reduced into S (finish_precond). levels 1: one spectral solve at
 // node_d[0]; levels 3: the reference's bank inside damped Jacobi sweeps (flexure.rs:1630-1651).
 template <class T>
@@ -1575,21 +1570,24 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
     return;
   }
   launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, r, L.left, L.S, st);  // left = r - A(J r)
-  // part = sum_k w_k S_k(w_k left): the three levels' transforms are independent, so levels 1 and
-  // 2 run on side streams (parallel branches when captured into the loop graph) into their own
-  // buffers, summed before the final pass
+  // part = sum_k w_k S_k(w_k left): the three levels' forward transforms and column passes are
+  // independent, so levels 1 and 2 run on side streams (parallel branches when captured into the
+  // loop graph); one inverse pass then takes the three spectra to the weighted sum
   cudaEventRecord(s->ev_fork, st);
   cudaStreamWaitEvent(s->side[0], s->ev_fork, 0);
   cudaStreamWaitEvent(s->side[1], s->ev_fork, 0);
-  launch_spectral<T>(s, L, L.left, L.wt[0], L.part, INV_STORE_W, 0, L.S, st);
-  launch_spectral<T>(s, L, L.left, L.wt[1], L.part_side[0], INV_STORE_W, 1, L.S, s->side[0], L.half_side[0]);
-  launch_spectral<T>(s, L, L.left, L.wt[2], L.part_side[1], INV_STORE_W, 2, L.S, s->side[1], L.half_side[1]);
+  FftGeo g = fft_geometry<T>(s);
+  cudaStream_t lst[3] = {st, s->side[0], s->side[1]};
+  cplx<T>* lh[3] = {L.half, L.half_side[0], L.half_side[1]};
+  for (int k = 0; k < 3; ++k) {
+    launch_rows_fwd<T>(s, L, L.left, L.wt[k], lh[k], g, L.S, lst[k]);
+    launch_cols<T>(s, L, lh[k], g, k, L.S, lst[k]);
+  }
   cudaEventRecord(s->ev_join[0], s->side[0]);
   cudaEventRecord(s->ev_join[1], s->side[1]);
   cudaStreamWaitEvent(st, s->ev_join[0], 0);
   cudaStreamWaitEvent(st, s->ev_join[1], 0);
-  k_sum3<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.part, L.part_side[0], L.part_side[1]);
-  counted();
+  launch_rows_inv<T>(s, L, INV_BANK, L.half, L.part, L.wt[0], nullptr, g, L.S, st);
   launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, r, z, L.S, st);  // z = u + J(r - A u)
 }
 
@@ -2532,7 +2530,7 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
       5 * e * n,  // Jacobi left: r, J, d, c in; left out
       6 * e * n,  // Jacobi final: r, J, part, d, c in; z out
       3 * e * n,  // rows forward weighted: left, w in; half out
-      4 * e * n,  // rows inverse accumulate: half, w, part in; part out
+      7 * e * n,  // rows inverse of the bank: three spectra, three weights in; part out
   };
   cudaEvent_t a, b;
   DT_CUDA(cudaEventCreate(&a));
@@ -2552,7 +2550,7 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
         case 6: launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, L.r, L.left, L.S, st); break;
         case 7: launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, L.r, L.z, L.S, st); break;
         case 8: launch_rows_fwd<T>(s, L, L.left, L.wt[0], L.half, g, L.S, st); break;
-        case 9: launch_rows_inv<T>(s, L, INV_ACCUM, L.half, L.part, L.wt[0], nullptr, g, L.S, st); break;
+        case 9: launch_rows_inv<T>(s, L, INV_BANK, L.half, L.part, L.wt[0], nullptr, g, L.S, st); break;
       }
     };
     one();  // warm
