@@ -73,6 +73,17 @@ __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * 
 template <class C>
 __device__ __forceinline__ C cmuli(C a) { return mk<C>(-a.y, a.x); }
 
+// Single precision: both parts in one paired FP32 instruction (sm_100's add / mul / fma on
+// float2), each part rounded as the scalar forms above round it (a - b as fma(b, -1, a), exact
+// but for the one rounding of the sum; products contracted into one fma, as the compiler
+// contracts the scalar forms).
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(-a.y, a.y), make_float2(b.y, b.x), __fmul2_rn(make_float2(a.x, a.x), b));
+}
+
 // ---- deterministic reductions -------------------------------------------------------------
 // A reducing kernel writes one partial per block (fixed grid, fixed in-block order); the last
 // block to finish (an atomic ticket) sums the partials in index order. The result therefore does
