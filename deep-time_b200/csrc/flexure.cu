@@ -264,11 +264,40 @@ __device__ __forceinline__ void stage_tile(T* dst, const T* __restrict__ src, in
 
 __device__ __forceinline__ bool aligned16(const void* p) { return ((size_t)p & 15) == 0; }
 
-template <class T, int MODE>
+// A row's couplings on the sphere's metric (RowMetric, flexure.rs:954-998): east-west a_j, the
+// boundaries above and below b_j, b_(j+1); rows outside the raster take the edge row's.
+template <class T, bool MET>
+struct RowCoef {
+  T a, bn, bs;
+};
+template <class T, bool MET>
+__device__ __forceinline__ RowCoef<T, MET> row_coef(const T* __restrict__ ma, const T* __restrict__ mb, int j, int h) {
+  RowCoef<T, MET> r{(T)1, (T)1, (T)1};
+  if (MET) {
+    const int jc = min(max(j, 0), h - 1);
+    r.a = ma[jc];
+    r.bn = mb[jc];
+    r.bs = mb[jc + 1];
+  }
+  return r;
+}
+// The 5-point Laplacian of cell x from its west, east, north and south neighbours: the block
+// metric's (flexure.rs:1575-1580), or the sphere's a (W + E - 2x) + bn (N - x) + bs (S - x)
+// (flexure.rs:1559-1570), in the reference's order of operations.
+template <class T, bool MET>
+__device__ __forceinline__ T lap5(T we, T ea, T no, T so, T x, const RowCoef<T, MET>& k, T inv) {
+  if (MET) return (k.a * (we + ea - (T)2 * x) + k.bn * (no - x) + k.bs * (so - x)) * inv;
+  return (we + ea + no + so - (T)4 * x) * inv;
+}
+
+// MET: on the sphere's row metric (ma: h values a_j, mb: h + 1 values b_j); the block metric
+// otherwise.
+template <class T, int MODE, bool MET = false>
 __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, const T* __restrict__ v, const T* __restrict__ J,
                                                     const T* __restrict__ part, const T* __restrict__ d,
                                                     const T* __restrict__ c, const T* __restrict__ rb, T* __restrict__ y,
-                                                    double* partials, Scalars* S) {
+                                                    double* partials, Scalars* S, const T* __restrict__ ma = nullptr,
+                                                    const T* __restrict__ mb = nullptr) {
   if (MODE != PLAIN && MODE != BEND && MODE != RESID) {
     if (S->stop) {
       if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0 && threadIdx.y == 0) set_cond(S, 0);
@@ -333,7 +362,8 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
       int lr = a + q;
       if (q == SEG && !(ty == 0 || ty == TTY - 1)) break;
       T us = ucol[(lr + 3) * P];
-      T lap = (ucol[(lr + 2) * P - 1] + ucol[(lr + 2) * P + 1] + un + us - (T)4 * uc) * inv_dx2;
+      T lap = lap5<T, MET>(ucol[(lr + 2) * P - 1], ucol[(lr + 2) * P + 1], un, us, uc, row_coef<T, MET>(ma, mb, j0 + lr, h),
+                           inv_dx2);
       mcol[(lr + 1) * P] = lap * mcol[(lr + 1) * P];
       un = uc;
       uc = us;
@@ -343,7 +373,7 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
   for (int e = tid; e < 2 * MR; e += TBX * TTY) {
     int lr = (e >> 1) - 1, lc = (e & 1) ? TBX : -1;
     const T* uc = su + (lr + 2) * P + OFF + lc;
-    T lap = (uc[-1] + uc[1] + uc[-P] + uc[P] - (T)4 * uc[0]) * inv_dx2;
+    T lap = lap5<T, MET>(uc[-1], uc[1], uc[-P], uc[P], uc[0], row_coef<T, MET>(ma, mb, j0 + lr, h), inv_dx2);
     T* m = sd + (lr + 1) * P + OFF + lc;
     *m = lap * *m;
   }
@@ -370,7 +400,8 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply(int w, int h, T inv_dx2, con
     for (int q = 0; q < SEG; ++q) {
       const int lr = r0 + q;
       T ms = mcol[(lr + 2) * P];
-      T lm = (mcol[(lr + 1) * P - 1] + mcol[(lr + 1) * P + 1] + mn + ms - (T)4 * mc) * inv_dx2;
+      T lm = lap5<T, MET>(mcol[(lr + 1) * P - 1], mcol[(lr + 1) * P + 1], mn, ms, mc, row_coef<T, MET>(ma, mb, j0 + lr, h),
+                          inv_dx2);
       mn = mc;
       mc = ms;
       int j = j0 + lr;
@@ -630,7 +661,9 @@ __global__ void __launch_bounds__(256) k_stats(size_t n, const T* __restrict__ d
 template <class T>
 __global__ void __launch_bounds__(256) k_bank_weights(int w, int h, const T* __restrict__ d, const T* __restrict__ c, double dx,
                                                       T* __restrict__ w0, T* __restrict__ w1, T* __restrict__ w2,
-                                                      T* __restrict__ jac, const Scalars* S) {
+                                                      T* __restrict__ jac, const Scalars* S,
+                                                      const double* __restrict__ ma = nullptr,
+                                                      const double* __restrict__ mb = nullptr) {
   const double RHO_MANTLE = 3300.0;
   size_t n = (size_t)w * h;
   double lo = S->lo, hi = S->hi;
@@ -648,8 +681,16 @@ __global__ void __launch_bounds__(256) k_bank_weights(int w, int h, const T* __r
     w2[k] = (T)(k0 == 1 ? b : 0.0);
     double east = (double)d[(size_t)j * w + (i + 1) % w], west = (double)d[(size_t)j * w + (i + w - 1) % w];
     double north = (double)d[(size_t)max(j - 1, 0) * w + i], south = (double)d[(size_t)min(j + 1, h - 1) * w + i];
-    double around = east + west + north + south;
-    jac[k] = (T)(0.5 / ((double)c[k] + (16.0 * dv + around) * inv4));
+    if (ma) {
+      // (L D L)'s diagonal on the sphere's row metric (flexure.rs:1444-1452)
+      double a = ma[j], bn = mb[j], bs = mb[j + 1];
+      double centre = 2.0 * a + bn + bs;
+      double diag = dv * centre * centre + (east + west) * a * a + north * bn * bn + south * bs * bs;
+      jac[k] = (T)(0.5 / ((double)c[k] + diag * inv4));
+    } else {
+      double around = east + west + north + south;
+      jac[k] = (T)(0.5 / ((double)c[k] + (16.0 * dv + around) * inv4));
+    }
   }
 }
 
@@ -943,6 +984,142 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   }
 }
 
+// The column pass on the sphere's row metric (RowSolve::solve, flexure.rs:1012-1099): no
+// transform along y; per wavenumber k the pentadiagonal d L_k^2 + c (L_k: diagonal
+// (a_j lx_k - b_j - b_(j+1)) / dx^2, off the diagonal b_(j+1) / dx^2) is factored as L D L^T
+// and solved, with the reference's recurrences and order of operations. The factors depend only
+// on the level's (d, c) and k, so k_row_factor makes them once per solve (dd, l1, l2: h x (N + 1)
+// each, row-major, wavenumber fastest) and k_row_solve does the substitutions at every
+// application. One thread per wavenumber q = 0 .. N; column q of the packed half spectrum holds
+// wavenumber q (both parts) for 0 < q < N, and column 0 wavenumbers 0 (real part) and N
+// (imaginary part), which threads 0 and N solve part by part.
+template <class T>
+__global__ void __launch_bounds__(128) k_row_factor(int N, int h, const T* __restrict__ lx, const T* __restrict__ ma,
+                                                    const T* __restrict__ mb, T inv_dx2, const Scalars* S, int level,
+                                                    T* __restrict__ dds, T* __restrict__ l1s, T* __restrict__ l2s) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > N) return;
+  const T d = (T)S->node_d[level], c = (T)S->c_ref;
+  const T lxk = lx[q];
+  const size_t stride = (size_t)N + 1;
+  T dd1 = 0, dd2 = 0, l1p = 0;  // dd[j-1], dd[j-2], l1[j-1]
+  T t1 = 0, e1 = 0, e2 = 0;     // t(j-1), e(j-1), e(j-2)
+#pragma unroll 4
+  for (int j = 0; j < h; ++j) {
+    const T tj = (ma[j] * lxk - mb[j] - mb[j + 1]) * inv_dx2;
+    const T ej = j + 1 < h ? mb[j + 1] * inv_dx2 : (T)0;
+    T p1 = 0, p2 = 0;
+    if (j >= 2) p2 = d * e2 * e1 / dd2;  // m2(j-2) / dd[j-2]
+    if (j >= 1) {
+      T carried = j >= 2 ? p2 * dd2 * l1p : (T)0;
+      p1 = (d * e1 * (t1 + tj) - carried) / dd1;  // (m1(j-1) - carried) / dd[j-1]
+    }
+    const T up = j > 0 ? e1 : (T)0;
+    T dj = d * (tj * tj + up * up + ej * ej) + c;  // m0(j)
+    if (j >= 1) dj -= p1 * p1 * dd1;
+    if (j >= 2) dj -= p2 * p2 * dd2;
+    dds[(size_t)j * stride + q] = dj;
+    l1s[(size_t)j * stride + q] = p1;
+    l2s[(size_t)j * stride + q] = p2;
+    dd2 = dd1;
+    dd1 = dj;
+    l1p = p1;
+    e2 = e1;
+    e1 = ej;
+    t1 = tj;
+  }
+}
+
+// The substitutions: x[j] -= x[j-1] l1[j] + ... going down, x[j] /= dd[j], x[j] -= x[j+1] l1[j+1]
+// + ... going up, in place on the level's spectrum. A thread's recurrence waits on nothing but
+// its own arithmetic: it loads RB rows (spectrum and factors) at a time before walking them.
+template <class T>
+__global__ void __launch_bounds__(128) k_row_solve(int N, int h, cplx<T>* __restrict__ half, const T* __restrict__ dds,
+                                                   const T* __restrict__ l1s, const T* __restrict__ l2s, const Scalars* S) {
+  using C = cplx<T>;
+  constexpr int RB = 8;
+  if (S->stop) return;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > N) return;
+  const int col = q == N ? 0 : q;
+  const bool re = q != N, im = q != 0;  // the parts this thread owns
+  const size_t stride = (size_t)N + 1;
+  auto store = [&](int j, C v) {
+    // column 0's parts belong to two threads: each stores only its own
+    if (re && im) {
+      half[(size_t)j * N + col] = v;
+    } else if (re) {
+      half[(size_t)j * N + col].x = v.x;
+    } else {
+      half[(size_t)j * N + col].y = v.y;
+    }
+  };
+  C x1 = mk<C>((T)0, (T)0), x2 = x1;  // x'[j-1], x'[j-2] (before the division)
+  for (int j0 = 0; j0 < h; j0 += RB) {
+    C v[RB];
+    T a1[RB], a2[RB], dv[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = min(j0 + u, h - 1);
+      v[u] = half[(size_t)j * N + col];
+      a1[u] = l1s[(size_t)j * stride + q];
+      a2[u] = l2s[(size_t)j * stride + q];
+      dv[u] = dds[(size_t)j * stride + q];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = j0 + u;
+      if (j >= h) break;
+      C x = v[u];
+      if (j >= 1) {
+        x.x -= x1.x * a1[u];
+        x.y -= x1.y * a1[u];
+      }
+      if (j >= 2) {
+        x.x -= x2.x * a2[u];
+        x.y -= x2.y * a2[u];
+      }
+      x2 = x1;
+      x1 = x;
+      store(j, mk<C>(x.x / dv[u], x.y / dv[u]));
+    }
+  }
+  // the walk up: x[j] -= x[j+1] l1[j+1]; x[j] -= x[j+2] l2[j+2]
+  C y1 = mk<C>((T)0, (T)0), y2 = y1;  // x[j+1], x[j+2]
+  T l1n = 0, l2n = 0, l2nn = 0;       // l1[j+1], l2[j+1], l2[j+2]
+  for (int j0 = h - 1; j0 >= 0; j0 -= RB) {
+    C v[RB];
+    T a1[RB], a2[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = max(j0 - u, 0);
+      v[u] = half[(size_t)j * N + col];
+      a1[u] = l1s[(size_t)j * stride + q];
+      a2[u] = l2s[(size_t)j * stride + q];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = j0 - u;
+      if (j < 0) break;
+      C x = v[u];
+      if (j + 1 < h) {
+        x.x -= y1.x * l1n;
+        x.y -= y1.y * l1n;
+      }
+      if (j + 2 < h) {
+        x.x -= y2.x * l2nn;
+        x.y -= y2.y * l2nn;
+      }
+      store(j, x);
+      y2 = y1;
+      y1 = x;
+      l2nn = l2n;
+      l1n = a1[u];
+      l2n = a2[u];
+    }
+  }
+}
+
 // Inverse rows: Z[k] = E[k] + i O[k] with E = (X[k] + conj X[N-k]) / 2,
 // O = (X[k] - conj X[N-k]) conj(W^k) / 2; x = IFFT_N(Z) / N de-interleaved.
 template <class T, int MODE, int LOGN>
@@ -1216,6 +1393,8 @@ struct Lane {
   // the bank's levels 1 and 2 transform beside level 0, into their own spectra: the three
   // spectra are consecutive (half + k h N), as are the three weights (wt[k] = wt[0] + k n)
   cplx<T>* half_side[2] = {nullptr, nullptr};
+  // the row metric's L D L^T factors per bank level: dd, l1, l2 (h x (N + 1) each)
+  T* row_factors = nullptr;
   Tables<T> tab;
   Scalars* S = nullptr;
   cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
@@ -1252,6 +1431,11 @@ struct dt_flex {
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
   // and box shape, made on first use
   bool tma = false;
+  // the sphere's row metric (RowMetric): a (h values) and b (h + 1) in both precisions; null for
+  // the block metric
+  bool metric = false;
+  double *met_a64 = nullptr, *met_b64 = nullptr;
+  float *met_a32 = nullptr, *met_b32 = nullptr;
   // the bank levels' side streams and their fork / join events
   cudaStream_t side[2] = {nullptr, nullptr};
   cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
@@ -1324,6 +1508,7 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   DT_TRY(dalloc(s, &L.half, 3 * hn));
   L.half_side[0] = L.half + hn;
   L.half_side[1] = L.half + 2 * hn;
+  if (s->metric) DT_TRY(dalloc(s, &L.row_factors, 9 * (size_t)s->h * (s->N + 1)));
   DT_TRY(make_tables(s, L.tab));
   DT_TRY(dalloc(s, &L.S, 1));
   DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
@@ -1339,6 +1524,19 @@ static void free_graphs(Lane<T>& L) {
     L.graph[k] = nullptr;
   }
 }
+
+template <class T>
+static const T* metric_a(const dt_flex* s);
+template <>
+const double* metric_a<double>(const dt_flex* s) { return s->met_a64; }
+template <>
+const float* metric_a<float>(const dt_flex* s) { return s->met_a32; }
+template <class T>
+static const T* metric_b(const dt_flex* s);
+template <>
+const double* metric_b<double>(const dt_flex* s) { return s->met_b64; }
+template <>
+const float* metric_b<float>(const dt_flex* s) { return s->met_b32; }
 
 static unsigned int ew_grid(const dt_flex* s) { return std::max(1u, std::min<unsigned int>(ceil_div(s->n, 256), (unsigned)s->sms * 8)); }
 
@@ -1422,10 +1620,32 @@ static bool launch_apply_tma(dt_flex* s, const T* vsrc, const T* J, const T* par
   return true;
 }
 
+// The operator on the sphere's row metric: the per-block kernel (the TMA stencil has the block
+// metric only), the handle's couplings in the lane's precision.
+template <class T>
+static void launch_apply_metric(dt_flex* s, int mode, dim3 grid, dim3 block, T inv, const T* v, const T* J, const T* part,
+                                const T* d, const T* c, const T* rb, T* y, Scalars* S, cudaStream_t st) {
+  const T* ma = metric_a<T>(s);
+  const T* mb = metric_b<T>(s);
+#define DT_MET_CASE(M) \
+  case M: k_apply<T, M, true><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S, ma, mb); break;
+  switch (mode) {
+    DT_MET_CASE(AP_DOT)
+    DT_MET_CASE(RESID)
+    DT_MET_CASE(JAC_LEFT)
+    DT_MET_CASE(JAC_FINAL)
+    DT_MET_CASE(PLAIN)
+    DT_MET_CASE(BEND)
+    DT_MET_CASE(RESID_GATED)
+  }
+#undef DT_MET_CASE
+  counted();
+}
+
 template <class T>
 static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* part, const T* d, const T* c, const T* rb, T* y,
                          Scalars* S, cudaStream_t st) {
-  if (s->tma) {
+  if (s->tma && !s->metric) {
     const T* vsrc = (mode == JAC_LEFT || mode == JAC_FINAL) ? rb : v;
     bool done = false;
     switch (mode) {
@@ -1441,6 +1661,10 @@ static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* 
   }
   dim3 grid(ceil_div(s->w, TBX), ceil_div(s->h, tile_rows<T>())), block(TBX, TTY);
   T inv = (T)(1.0 / (s->dx * s->dx));
+  if (s->metric) {
+    launch_apply_metric<T>(s, mode, grid, block, inv, v, J, part, d, c, rb, y, S, st);
+    return;
+  }
   switch (mode) {
     case AP_DOT: k_apply<T, AP_DOT><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
     case RESID: k_apply<T, RESID><<<grid, block, 0, st>>>(s->w, s->h, inv, v, J, part, d, c, rb, y, s->partials, S); counted(); break;
@@ -1537,6 +1761,14 @@ static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cp
 }
 template <class T>
 static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, int level, Scalars* S, cudaStream_t st) {
+  if (s->metric) {
+    // the row solve per wavenumber with the level's factors (made by setup_precond)
+    const size_t fac = (size_t)s->h * (s->N + 1);
+    const T* dd = L.row_factors + (size_t)level * 3 * fac;
+    k_row_solve<T><<<ceil_div(s->N + 1, 128), 128, 0, st>>>(s->N, s->h, half, dd, dd + fac, dd + 2 * fac, S);
+    counted();
+    return;
+  }
   cols_fn<T>(ilog2(s->h), LogSeq{})<<<g.cgrid, g.cthreads, g.csmem, st>>>(s->N, half, L.tab.tw_col, L.tab.omega, L.tab.lx,
                                                                           L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S, level);
   counted();
@@ -1726,8 +1958,19 @@ static dt_status setup_precond(dt_flex* s, Lane<T>& L, int precond, int* levels)
   DT_CUDA(cudaMemcpyAsync(&lv, &L.S->levels, sizeof(int), cudaMemcpyDeviceToHost, st));
   DT_CUDA(cudaStreamSynchronize(st));
   if (lv == 3) {
-    k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S);
+    k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S,
+                                                   s->met_a64, s->met_b64);
     counted();
+  }
+  if (s->metric) {
+    // the row solve's factors of each level (its d, the bank's c_ref)
+    const size_t fac = (size_t)s->h * (s->N + 1);
+    for (int k = 0; k < lv; ++k) {
+      T* dd = L.row_factors + (size_t)k * 3 * fac;
+      k_row_factor<T><<<ceil_div(s->N + 1, 128), 128, 0, st>>>(s->N, s->h, L.tab.lx, metric_a<T>(s), metric_b<T>(s),
+                                                             (T)(1.0 / (s->dx * s->dx)), L.S, k, dd, dd + fac, dd + 2 * fac);
+      counted();
+    }
   }
   DT_CUDA(cudaGetLastError());
   *levels = lv;
@@ -2121,13 +2364,28 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     set_error("dt_flex_create: bad raster %d x %d, dx %g", w, h, dx);
     return DT_BAD_ARG;
   }
-  if ((w & 1) || !is_pow2(w / 2) || !is_pow2(h) || w / 2 > 8192 || h > 8192) {
-    set_error("dt_flex_create: the device transforms need w/2 and h powers of two, at most 8192 (got %d x %d)", w, h);
+  // the cosine transform along y needs h a power of two; on the row metric y is solved per
+  // wavenumber instead, so any h will do
+  if ((w & 1) || !is_pow2(w / 2) || w / 2 > 8192 || h > 8192 || (!metric_a && !is_pow2(h))) {
+    set_error("dt_flex_create: the device transforms need w/2 (and, for the block metric, h) powers of two, at most "
+              "8192 (got %d x %d)", w, h);
     return DT_UNSUPPORTED;
   }
-  if (metric_a || metric_b) {
-    set_error("dt_flex_create: the sphere's row metric (RowMetric) has no device path in this build");
-    return DT_UNSUPPORTED;
+  if (!metric_a != !metric_b) {
+    set_error("dt_flex_create: the row metric needs both a (h values) and b (h + 1 values)");
+    return DT_BAD_ARG;
+  }
+  if (metric_a) {
+    for (int j = 0; j < h; ++j)
+      if (!std::isfinite(metric_a[j])) {
+        set_error("dt_flex_create: metric a[%d] is not finite", j);
+        return DT_BAD_ARG;
+      }
+    for (int j = 0; j <= h; ++j)
+      if (!std::isfinite(metric_b[j])) {
+        set_error("dt_flex_create: metric b[%d] is not finite", j);
+        return DT_BAD_ARG;
+      }
   }
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
@@ -2152,6 +2410,21 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     return fail(DT_DEVICE_ERROR);
   }
   s->own_stream = true;
+  if (metric_a) {
+    // the sphere's row metric (RowMetric, flexure.rs:954-998), in both lanes' precisions
+    s->metric = true;
+    std::vector<float> a32(metric_a, metric_a + h), b32(metric_b, metric_b + h + 1);
+    if ((st = dalloc(s, &s->met_a64, (size_t)h)) != DT_OK || (st = dalloc(s, &s->met_b64, (size_t)h + 1)) != DT_OK ||
+        (st = dalloc(s, &s->met_a32, (size_t)h)) != DT_OK || (st = dalloc(s, &s->met_b32, (size_t)h + 1)) != DT_OK)
+      return fail(st);
+    if (cudaMemcpy(s->met_a64, metric_a, h * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->met_b64, metric_b, (h + 1) * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->met_a32, a32.data(), h * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(s->met_b32, b32.data(), (h + 1) * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("dt_flex_create: metric upload failed");
+      return fail(DT_DEVICE_ERROR);
+    }
+  }
   if ((st = make_lane<double>(s, s->L64)) != DT_OK) return fail(st);
   if ((st = make_lane<float>(s, s->L32)) != DT_OK) return fail(st);
   if ((st = dalloc(s, &s->b64, s->n)) != DT_OK) return fail(st);
@@ -2166,7 +2439,7 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   {
     // the TMA stencil takes rasters whose rows are whole tiles; DT_STENCIL_TMA=0 turns it off
     const char* env = getenv("DT_STENCIL_TMA");
-    s->tma = w % TBX == 0 && encode_tiled() != nullptr && !(env && env[0] == '0');
+    s->tma = w % TBX == 0 && !s->metric && encode_tiled() != nullptr && !(env && env[0] == '0');
     if (s->tma) {
       tma_setup_all<double>();
       tma_setup_all<float>();

@@ -97,7 +97,11 @@ typedef struct dt_diff dt_diff;
 void dt_flex_default_params(dt_flex_params* p);
 
 /* metric_a (h values) and metric_b (h + 1 values) select the sphere's row metric (RowMetric,
- * flexure.rs:964-1010); pass NULL for the block metric. */
+ * flexure.rs:954-1010, Solver::with_metric :1528); pass NULL for both for the block metric, and
+ * one without the other is DT_BAD_ARG. On the row metric the operator runs the per-block stencil
+ * with the rows' couplings, the Jacobi weights take (L D L)'s diagonal on the metric, and the
+ * spectral pass solves d L_k^2 + c per wavenumber along y (RowSolve, :1012-1099) in place of the
+ * cosine transform, so h need not be a power of two (w/2 still must). */
 dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const double* metric_b, dt_flex** out);
 dt_status dt_flex_destroy(dt_flex* s);
 /* Binds the handle to a CUDA stream (cudaStream_t passed as void*); NULL = the handle's own. */
