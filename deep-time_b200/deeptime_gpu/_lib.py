@@ -67,6 +67,11 @@ def lib():
         L.dt_flex_profile_kernels.argtypes = [vp, i, i, vp, vp]
         L.dt_flex_set_unet.argtypes = [vp, vp, d]
         L.dt_flex_operator_dot_noalloc.argtypes = [i, i, d, vp, vp, vp, vp, vp, vp]
+        L.dt_grid_restrict_dev.argtypes = [i, i, i, vp, vp, vp]
+        L.dt_grid_prolong_const_dev.argtypes = [i, i, i, vp, vp, vp]
+        L.dt_grid_prolong_linear_dev.argtypes = [i, i, i, vp, vp, vp]
+        L.dt_grid_binomial_dev.argtypes = [i, i, i, vp, vp, vp]
+        L.dt_grid_box_blur_dev.argtypes = [i, i, i, i, i, vp, vp, vp]
         _lib = L
     return _lib
 

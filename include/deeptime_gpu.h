@@ -201,6 +201,27 @@ dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
 #define DT_PROFILE_KERNELS 10
 dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes);
 
+/* The flexure step's grid helpers on device arrays (row-major, x fastest), enqueued on `stream`
+ * (NULL: the legacy default stream) without a host sync; each result is bit-for-bit the
+ * reference's.
+ *   restrict:       coarse (w/f x h/f) = the mean of each f x f block of fine (w x h); the
+ *                   cells of a block summed row by row, then times 1/(f f); f = 1 copies
+ *                   (restrict_by, flexure.rs:1773-1795).
+ *   prolong_const:  fine (ws f x hs f) = each coarse cell's value on its f x f cells
+ *                   (coarse_cell / prolong_const, flexure.rs:1797-1813).
+ *   prolong_linear: fine = bilinear interpolation from the coarse cells' centres, x wrapping,
+ *                   rows clamped (prolong_linear / linear_at, flexure.rs:1815-1844).
+ *   binomial:       `passes` of [1/4, 1/2, 1/4] along x (wrapping) then y (rows clamped), in
+ *                   place; scratch holds w h values (binomial, flexure.rs:1745-1762).
+ *   box_blur:       `passes` of the radius-r running-sum box along x (wrapping when wrap_x,
+ *                   else clamped) then y (rows reflected), in place; scratch holds w h values
+ *                   (box_blur, grid.rs:224-270). */
+dt_status dt_grid_restrict_dev(int w, int h, int f, const double* fine, double* coarse, void* stream);
+dt_status dt_grid_prolong_const_dev(int ws, int hs, int f, const double* coarse, double* fine, void* stream);
+dt_status dt_grid_prolong_linear_dev(int ws, int hs, int f, const double* coarse, double* fine, void* stream);
+dt_status dt_grid_binomial_dev(int w, int h, int passes, double* v, double* scratch, void* stream);
+dt_status dt_grid_box_blur_dev(int w, int h, int wrap_x, int r, int passes, double* v, double* scratch, void* stream);
+
 const char* dt_last_error(void);
 /* Library and device facts: 1 when a CUDA device is usable, with its name. */
 int dt_device_info(char* name, int len);

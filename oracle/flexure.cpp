@@ -592,6 +592,77 @@ void box_blur(size_t w, size_t h, bool wrap, double* v, size_t r, size_t passes)
   }
 }
 
+// surface/flexure.rs:1773-1795 (restrict_by): the mean of each f x f block, its cells summed
+// row by row, then times 1 / (f f); a copy where f = 1.
+void restrict_by(size_t w, size_t h, size_t f, const double* v, double* out) {
+  if (f == 1) {
+    std::copy(v, v + w * h, out);
+    return;
+  }
+  size_t ws = w / f, hs = h / f;
+  double norm = 1.0 / (double)(f * f);
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < (long)(ws * hs); ++c) {
+    size_t i = (size_t)c % ws, j = (size_t)c / ws;
+    double s = 0.0;
+    for (size_t dj = 0; dj < f; ++dj)
+      for (size_t di = 0; di < f; ++di) s += v[(j * f + dj) * w + i * f + di];
+    out[c] = s * norm;
+  }
+}
+
+// surface/flexure.rs:1797-1813 (coarse_cell, prolong_const): each coarse value on its f x f cells.
+void prolong_const(size_t ws, size_t hs, size_t f, const double* v, double* out) {
+  size_t w = ws * f, n = w * hs * f;
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < (long)n; ++c) {
+    size_t i = (size_t)c % w, j = (size_t)c / w;
+    out[c] = v[(j / f) * ws + i / f];
+  }
+}
+
+// surface/flexure.rs:1815-1844 (prolong_linear, linear_at): bilinear from the coarse cells'
+// centres, x wrapping, rows clamped.
+void prolong_linear(size_t ws, size_t hs, size_t f, const double* v, double* out) {
+  size_t w = ws * f, n = w * hs * f;
+  if (f == 1) {
+    std::copy(v, v + n, out);
+    return;
+  }
+#pragma omp parallel for schedule(static)
+  for (long c = 0; c < (long)n; ++c) {
+    size_t i = (size_t)c % w, j = (size_t)c / w;
+    double x = ((double)i + 0.5) / (double)f - 0.5;
+    double y = std::clamp(((double)j + 0.5) / (double)f - 0.5, 0.0, (double)(hs - 1));
+    double x0 = std::floor(x), y0 = std::floor(y);
+    double tx = x - x0, ty = y - y0;
+    long iw = (long)x0 % (long)ws;
+    size_t i0 = (size_t)(iw < 0 ? iw + (long)ws : iw), i1 = (i0 + 1) % ws;
+    size_t j0 = (size_t)y0, j1 = std::min(j0 + 1, hs - 1);
+    out[c] = (v[j0 * ws + i0] * (1.0 - tx) + v[j0 * ws + i1] * tx) * (1.0 - ty) +
+             (v[j1 * ws + i0] * (1.0 - tx) + v[j1 * ws + i1] * tx) * ty;
+  }
+}
+
+// surface/flexure.rs:1745-1762 (binomial): passes of the [1/4, 1/2, 1/4] filter along x
+// (wrapping) then along y (rows clamped).
+void binomial(size_t w, size_t h, size_t passes, double* v) {
+  std::vector<double> tmp(w * h);
+  for (size_t pass = 0; pass < passes; ++pass) {
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < (long)h; ++j)
+      for (size_t i = 0; i < w; ++i) {
+        const double* row = v + j * w;
+        tmp[j * w + i] = 0.25 * row[(i + w - 1) % w] + 0.5 * row[i] + 0.25 * row[(i + 1) % w];
+      }
+#pragma omp parallel for schedule(static)
+    for (long j = 0; j < (long)h; ++j) {
+      size_t n = j > 0 ? (size_t)j - 1 : 0, s = std::min((size_t)j + 1, h - 1);
+      for (size_t i = 0; i < w; ++i) v[j * w + i] = 0.25 * tmp[n * w + i] + 0.5 * tmp[j * w + i] + 0.25 * tmp[s * w + i];
+    }
+  }
+}
+
 }  // namespace oracle
 
 using namespace oracle;
@@ -662,5 +733,9 @@ void dto_row_metric_from_sin_faces(const double* sin_faces, int nfaces, int f, d
 }
 
 void dto_box_blur(int w, int h, int wrap, double* v, int r, int passes) { box_blur(w, h, wrap != 0, v, r, passes); }
+void dto_restrict_by(int w, int h, int f, const double* v, double* out) { restrict_by(w, h, f, v, out); }
+void dto_prolong_const(int ws, int hs, int f, const double* v, double* out) { prolong_const(ws, hs, f, v, out); }
+void dto_prolong_linear(int ws, int hs, int f, const double* v, double* out) { prolong_linear(ws, hs, f, v, out); }
+void dto_binomial(int w, int h, int passes, double* v) { binomial(w, h, passes, v); }
 
 }  // extern "C"

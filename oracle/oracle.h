@@ -31,6 +31,10 @@ int dto_flex_solve(int w, int h, double dx, const double* ma, const double* mb, 
                    double* x, double tol, int max_it, int precond, int stop, dto_report* rep);
 void dto_row_metric_from_sin_faces(const double* sin_faces, int nfaces, int f, double* a, double* b);
 void dto_box_blur(int w, int h, int wrap, double* v, int r, int passes);
+void dto_restrict_by(int w, int h, int f, const double* v, double* out);
+void dto_prolong_const(int ws, int hs, int f, const double* v, double* out);
+void dto_prolong_linear(int ws, int hs, int f, const double* v, double* out);
+void dto_binomial(int w, int h, int passes, double* v);
 
 int dto_diff_operator(int w, int h, double dx, int wrap, const double* kd, double dt, const double* x, double* y);
 int dto_diff_operator_coeffs(int w, int h, double dx, int wrap, const double* kd, double dt, double* east, double* south,

@@ -152,6 +152,41 @@ def box_blur(v, r, passes, wrap=True):
     return v
 
 
+def restrict_by(v, f):
+    """flexure.rs:1773-1795: the mean of each f x f block."""
+    v = _f64(v)
+    h, w = v.shape
+    out = np.empty((h // f, w // f))
+    lib().dto_restrict_by(w, h, f, _p(v), _p(out))
+    return out
+
+
+def prolong_const(v, f):
+    """flexure.rs:1803-1813."""
+    v = _f64(v)
+    hs, ws = v.shape
+    out = np.empty((hs * f, ws * f))
+    lib().dto_prolong_const(ws, hs, f, _p(v), _p(out))
+    return out
+
+
+def prolong_linear(v, f):
+    """flexure.rs:1816-1844: bilinear from the coarse cells' centres, x wrapping, rows clamped."""
+    v = _f64(v)
+    hs, ws = v.shape
+    out = np.empty((hs * f, ws * f))
+    lib().dto_prolong_linear(ws, hs, f, _p(v), _p(out))
+    return out
+
+
+def binomial(v, passes):
+    """flexure.rs:1745-1762: [1/4, 1/2, 1/4] along x (wrapping), then y (rows clamped)."""
+    v = _f64(v).copy()
+    h, w = v.shape
+    lib().dto_binomial(w, h, passes, _p(v))
+    return v
+
+
 def diff_operator(x, kd, dt, dx, wrap=True):
     h, w = x.shape
     x, kd = _f64(x), _f64(kd)
