@@ -1,8 +1,9 @@
 /* Test infrastructure only: the C interface of the CPU oracle (a restatement of the reference's
- * CPU solvers; see flexure.cpp and diffusion.cpp for the file:line each function follows). Only
+ * CPU solvers; see flexure.cpp, diffusion.cpp and cube.cpp for the file:line each function follows). Only
  * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load liboracle.so. */
 #ifndef DEEPTIME_ORACLE_H
 #define DEEPTIME_ORACLE_H
+#include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -35,6 +36,18 @@ void dto_restrict_by(int w, int h, int f, const double* v, double* out);
 void dto_prolong_const(int ws, int hs, int f, const double* v, double* out);
 void dto_prolong_linear(int ws, int hs, int f, const double* v, double* out);
 void dto_binomial(int w, int h, int passes, double* v);
+
+/* The cube grid's diffusion (surface/cube/diffusion.rs, surface/cube/multigrid.rs): slots are
+ * 6 n^2 x 8 neighbour indices (0xFFFFFFFF: none), lap 6 n^2 x 8 coupling weights, areas 6 n^2. */
+void dto_cube_topology(int n, uint32_t* slots);
+void dto_cube_operator(int n, const uint32_t* slots, const double* lap, const double* areas, const double* kd, double dt,
+                       const double* x, double* y);
+void dto_cube_vcycle(int n, const uint32_t* slots, const double* lap, const double* areas, const double* kd, double dt,
+                     const double* r, double* z);
+void dto_cube_lod(int n, const uint32_t* slots, const double* lap, const double* areas, const double* kd, double dt,
+                  const double* h, double* x);
+int dto_cube_diff_solve(int n, const uint32_t* slots, const double* lap, const double* areas, const double* kd, double dt,
+                        double tol_m, double* h);
 
 int dto_diff_operator(int w, int h, double dx, int wrap, const double* kd, double dt, const double* x, double* y);
 int dto_diff_operator_coeffs(int w, int h, double dx, int wrap, const double* kd, double dt, double* east, double* south,

@@ -187,6 +187,52 @@ def binomial(v, passes):
     return v
 
 
+NO_CELL = 0xFFFFFFFF
+
+
+def cube_topology(n):
+    """sphere/cube.rs:76-93: the 6 n^2 cells' eight neighbour slots (E, NE, N, NW, W, SW, S, SE)."""
+    slots = np.zeros((6 * n * n, 8), dtype=np.uint32)
+    lib().dto_cube_topology(n, _p(slots))
+    return slots
+
+
+def _cube_args(n, slots, lap, areas, kd):
+    return (np.ascontiguousarray(slots, dtype=np.uint32), _f64(lap), _f64(areas), _f64(kd))
+
+
+def cube_operator(n, slots, lap, areas, kd, dt, x):
+    slots, lap, areas, kd = _cube_args(n, slots, lap, areas, kd)
+    x = _f64(x)
+    y = np.empty_like(x)
+    lib().dto_cube_operator(n, _p(slots), _p(lap), _p(areas), _p(kd), D(dt), _p(x), _p(y))
+    return y
+
+
+def cube_vcycle(n, slots, lap, areas, kd, dt, r):
+    slots, lap, areas, kd = _cube_args(n, slots, lap, areas, kd)
+    r = _f64(r)
+    z = np.empty_like(r)
+    lib().dto_cube_vcycle(n, _p(slots), _p(lap), _p(areas), _p(kd), D(dt), _p(r), _p(z))
+    return z
+
+
+def cube_lod(n, slots, lap, areas, kd, dt, h):
+    slots, lap, areas, kd = _cube_args(n, slots, lap, areas, kd)
+    h = _f64(h)
+    x = np.empty_like(h)
+    lib().dto_cube_lod(n, _p(slots), _p(lap), _p(areas), _p(kd), D(dt), _p(h), _p(x))
+    return x
+
+
+def cube_diff_solve(n, slots, lap, areas, kd, dt, tol_m, h):
+    """surface/cube/diffusion.rs::solve with DiffusionSolver::Multigrid; returns (h', iterations)."""
+    slots, lap, areas, kd = _cube_args(n, slots, lap, areas, kd)
+    h = _f64(h).copy()
+    its = lib().dto_cube_diff_solve(n, _p(slots), _p(lap), _p(areas), _p(kd), D(dt), D(tol_m), _p(h))
+    return h, its
+
+
 def diff_operator(x, kd, dt, dx, wrap=True):
     h, w = x.shape
     x, kd = _f64(x), _f64(kd)

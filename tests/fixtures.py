@@ -64,3 +64,29 @@ def rms(a, b):
 
 
 SIZES = [(1, 1), (1, 7), (7, 1), (2, 2), (2, 5), (3, 5), (5, 3), (17, 9), (33, 33), (64, 40), (129, 67), (200, 96)]
+
+
+def cube_case(n, seed, slots):
+    """A seeded cube-grid geometry for the cube diffusion's parity tests: cell areas within 20% of
+    each other and coupling weights symmetric across every pair (as CubeGrid::lap is: each pair
+    takes the value its lower-indexed cell computed, sphere/cube.rs:300-316), side pairs near 1,
+    diagonal pairs small, plus a diffusivity field with a sharp land-sea edge."""
+    rng = np.random.default_rng(seed)
+    cells = 6 * n * n
+    areas = 1.0 + 0.2 * rng.random(cells)
+    lap = np.zeros((cells, 8))
+    raw = np.where(np.arange(8) % 2 == 0, 0.8 + 0.4 * rng.random((cells, 8)), 0.05 + 0.15 * rng.random((cells, 8)))
+    none = slots == 0xFFFFFFFF
+    for c in range(cells):
+        for k in range(8):
+            m = int(slots[c, k])
+            if none[c, k]:
+                continue
+            if m > c:
+                lap[c, k] = raw[c, k]
+            else:
+                km = int(np.nonzero(slots[m] == c)[0][0])
+                lap[c, k] = raw[m, km]
+    kd = np.where(rng.random(cells) < 0.3, 0.02, 1.0) * (0.5 + rng.random(cells))
+    h = 1000.0 * rng.standard_normal(cells)
+    return lap, areas, kd, h
