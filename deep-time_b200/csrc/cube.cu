@@ -1,0 +1,854 @@
+// Implicit diffusion on the cube grid, preconditioned by one multigrid V-cycle, on the B200: the
+// device implementation behind dt_cube_* (include/deeptime_gpu.h) of the reference's
+// surface/cube/diffusion.rs::solve with DiffusionSolver::Multigrid and its V-cycle
+// (surface/cube/multigrid.rs):
+//
+//   k_cube_couplings  the operator (diffusion.rs:88-113, :147-240): per cell and neighbour slot
+//                     K = dt/mean_area D w, D the side pair's mean diffusivity or, for a diagonal,
+//                     the least of its quad's four side means; mu = area / mean_area; diag =
+//                     mu + sum K;
+//   k_cube_lod_*      the locally one-dimensional first guess (diffusion.rs:315-381): a Thomas
+//                     solve per face row, then per face column, couplings across a face's edge
+//                     at the old values;
+//   the hierarchy     2 x 2 blocks of each face down to <= 64 cells (multigrid.rs:92-186), its
+//                     sparsity built on the host once per grid (create), its values per solve on
+//                     the device (k_mg_val0, k_mg_valc, k_mg_mass);
+//   the V-cycle       damped Jacobi (omega 0.8, two sweeps before and after, the first from
+//                     zero), residuals summed over blocks, the coarse correction handed to each
+//                     block's cells, 16 sweeps on the coarsest level, all in FP32 with the
+//                     reference's products and sums (no fused multiply-adds), so it is the
+//                     oracle's cycle bit for bit;
+//   CG                FP64, the reference's two passes an iteration (the direction fused with
+//                     A p and p.Ap; x, r and r.r), stop at an RMS residual of tol over every cell
+//                     or after 400 iterations, then the residual's sum put back in proportion to
+//                     each cell's coupling (diffusion.rs:387-500, :283-301).
+//
+// The grid's geometry (neighbour slots, the coupling Laplacian's weights, the cell areas) comes
+// from the caller's CubeGrid at create. The CG loop is driven from the host (three scalars read
+// back an iteration).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "common.cuh"
+
+namespace dt {
+
+constexpr uint32_t CUBE_NO_CELL = 0xFFFFFFFFu;
+constexpr float CUBE_OMEGA = 0.8f;     // diffusion/multigrid.rs:45
+constexpr int CUBE_NU = 2;             // multigrid.rs:48
+constexpr float CUBE_SCALE = 0.5f;     // multigrid.rs:52
+constexpr size_t CUBE_COARSEST = 64;   // multigrid.rs:54
+constexpr int CUBE_COARSE_SWEEPS = 16; // multigrid.rs:56
+constexpr int CUBE_CG_MAX_ITER = 400;  // surface/diffusion.rs:497
+constexpr int CUBE_RED_BLOCKS = 592;   // partial sums per reduction (4 per SM)
+
+// ---- the operator ----
+__global__ void k_cube_couplings(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ lap,
+                                 const double* __restrict__ kd, const double* __restrict__ mu, double scale,
+                                 double* __restrict__ k, double* __restrict__ s, double* __restrict__ diag) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t* sl = slots + c * 8;
+    auto m2 = [&](size_t x, size_t y) { return __dmul_rn(0.5, __dadd_rn(kd[x], kd[y])); };
+    double sum = 0.0;
+    for (int slot = 0; slot < 8; ++slot) {
+      const uint32_t m = sl[slot];
+      double kv = 0.0;
+      if (m != CUBE_NO_CELL) {
+        double d;
+        if ((slot & 1) == 0) {
+          d = m2(c, m);
+        } else {
+          const size_t a = sl[slot - 1], b = sl[(slot + 1) & 7];
+          d = fmin(fmin(fmin(m2(c, a), m2(a, m)), m2(m, b)), m2(b, c));
+        }
+        kv = __dmul_rn(__dmul_rn(scale, d), lap[c * 8 + slot]);
+      }
+      k[c * 8 + slot] = kv;
+      sum = __dadd_rn(sum, kv);
+    }
+    s[c] = sum;
+    diag[c] = __dadd_rn(mu[c], sum);
+  }
+}
+
+// The operator's row i: diag p_i - sum_slots K p_j
+template <class P>
+__device__ __forceinline__ double cube_row(size_t i, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                           const double* __restrict__ diag, P p) {
+  double acc = __dmul_rn(diag[i], p(i));
+  for (int t = 0; t < 8; ++t) {
+    const uint32_t j = slots[i * 8 + t];
+    if (j != CUBE_NO_CELL) acc = __dsub_rn(acc, __dmul_rn(k[i * 8 + t], p(j)));
+  }
+  return acc;
+}
+
+__global__ void k_cube_apply(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                             const double* __restrict__ diag, const double* __restrict__ x, double* __restrict__ y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x)
+    y[i] = cube_row(i, slots, k, diag, [&](size_t j) { return x[j]; });
+}
+
+// ---- deterministic sums: per-block partials in a fixed grid, then one block adds them in order ----
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double sh[32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) sh[warp] = v;
+  __syncthreads();
+  v = 0.0;
+  if (warp == 0) {
+    const int nw = (blockDim.x + 31) >> 5;
+    v = lane < nw ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  }
+  __syncthreads();
+  return v;  // thread 0 holds the block's sum
+}
+
+__global__ void k_cube_finish(int nparts, const double* __restrict__ partials, double* __restrict__ out) {
+  double v = 0.0;
+  for (int q = threadIdx.x; q < nparts; q += blockDim.x) v += partials[q];
+  v = block_sum(v);
+  if (threadIdx.x == 0) *out = v;
+}
+
+// r = rhs - A x; partial r.r
+__global__ void k_cube_resid(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                             const double* __restrict__ diag, const double* __restrict__ rhs, const double* __restrict__ x,
+                             double* __restrict__ r, double* __restrict__ partials) {
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    const double rv = __dsub_rn(rhs[i], cube_row(i, slots, k, diag, [&](size_t j) { return x[j]; }));
+    r[i] = rv;
+    acc += rv * rv;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// partial a.b
+__global__ void k_cube_dot(size_t cells, const double* __restrict__ a, const double* __restrict__ b, double* __restrict__ partials) {
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x)
+    acc += a[i] * b[i];
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// the direction pn = z + beta po (z alone on the first), A pn, partial pn.A pn (diffusion.rs:407-443)
+__global__ void k_cube_direction(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                 const double* __restrict__ diag, const double* __restrict__ z, const double* __restrict__ po,
+                                 const double* __restrict__ beta_p, int first, double* __restrict__ pn,
+                                 double* __restrict__ ap, double* __restrict__ partials) {
+  const double beta = first ? 0.0 : *beta_p;
+  auto dir = [&](size_t j) { return first ? z[j] : __dadd_rn(z[j], __dmul_rn(beta, po[j])); };
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    const double pi = dir(i);
+    const double a = cube_row(i, slots, k, diag, dir);
+    pn[i] = pi;
+    ap[i] = a;
+    acc += pi * a;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// x += alpha p; r -= alpha A p; partial r.r (diffusion.rs:448-475)
+__global__ void k_cube_update(size_t cells, const double* __restrict__ alpha_p, const double* __restrict__ p,
+                              const double* __restrict__ ap, double* __restrict__ x, double* __restrict__ r,
+                              double* __restrict__ partials) {
+  const double alpha = *alpha_p;
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    x[i] = __dadd_rn(x[i], __dmul_rn(alpha, p[i]));
+    const double rv = __dsub_rn(r[i], __dmul_rn(alpha, ap[i]));
+    r[i] = rv;
+    acc += rv * rv;
+  }
+  acc = block_sum(acc);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc;
+}
+
+// x += kk s / mu, the residual's sum put back (diffusion.rs:290-301)
+__global__ void k_cube_putback(size_t cells, const double* __restrict__ kk_p, const double* __restrict__ s,
+                               const double* __restrict__ mu, double* __restrict__ x) {
+  const double kk = *kk_p;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = __dadd_rn(x[i], __ddiv_rn(__dmul_rn(kk, s[i]), mu[i]));
+}
+
+// rhs = mu h; x = b = h
+__global__ void k_cube_start(size_t cells, const double* __restrict__ h, const double* __restrict__ mu,
+                             double* __restrict__ rhs, double* __restrict__ x, double* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    rhs[i] = __dmul_rn(mu[i], h[i]);
+    x[i] = h[i];
+    b[i] = h[i];
+  }
+}
+
+// ---- the LOD first guess (diffusion.rs:315-381, thomas :1029-1046) ----
+// One thread per face row: the tridiagonal (1 + (ke + kw)/mu, -kw/mu, -ke/mu) by Thomas, the
+// couplings across the face's west and east edges at b's values. cb: the Thomas coefficients.
+__global__ void k_cube_lod_rows(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                const double* __restrict__ mu, const double* __restrict__ b, double* __restrict__ x,
+                                double* __restrict__ cb) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= 6 * n) return;
+  const size_t c0 = (size_t)row * n;
+  auto di = [&](size_t c) { return __dadd_rn(1.0, __ddiv_rn(__dadd_rn(k[c * 8 + 0], k[c * 8 + 4]), mu[c])); };
+  auto rhs = [&](int i) {
+    const size_t c = c0 + i;
+    double v = b[c];
+    if (i == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 4], b[slots[c * 8 + 4]]), mu[c]));
+    if (i == n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 0], b[slots[c * 8 + 0]]), mu[c]));
+    return v;
+  };
+  double beta = di(c0);
+  double prev = __ddiv_rn(rhs(0), beta);
+  x[c0] = prev;
+  for (int i = 1; i < n; ++i) {
+    const size_t c = c0 + i;
+    const double up = __ddiv_rn(-k[(c - 1) * 8 + 0], mu[c - 1]);
+    const double lo = __ddiv_rn(-k[c * 8 + 4], mu[c]);
+    const double ci = __ddiv_rn(up, beta);
+    cb[c] = ci;
+    beta = __dsub_rn(di(c), __dmul_rn(lo, ci));
+    prev = __ddiv_rn(__dsub_rn(rhs(i), __dmul_rn(lo, prev)), beta);
+    x[c] = prev;
+  }
+  for (int i = n - 2; i >= 0; --i) {
+    const size_t c = c0 + i;
+    x[c] = __dsub_rn(x[c], __dmul_rn(cb[c + 1], x[c + 1]));
+  }
+}
+
+// One thread per face column: the same along j (N = slot 2, S = slot 6) from the rows' result
+// y, into out (column-major per face: column f n + i at out + (f n + i) n).
+__global__ void k_cube_lod_cols(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                const double* __restrict__ mu, const double* __restrict__ y, double* __restrict__ out,
+                                double* __restrict__ cb) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  if (col >= 6 * n) return;
+  const size_t nn = (size_t)n * n, f = col / n, i = col % n;
+  auto cell = [&](int j) { return f * nn + (size_t)j * n + i; };
+  auto di = [&](size_t c) { return __dadd_rn(1.0, __ddiv_rn(__dadd_rn(k[c * 8 + 2], k[c * 8 + 6]), mu[c])); };
+  auto rhs = [&](int j) {
+    const size_t c = cell(j);
+    double v = y[c];
+    if (j == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 2], y[slots[c * 8 + 2]]), mu[c]));
+    if (j == n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 6], y[slots[c * 8 + 6]]), mu[c]));
+    return v;
+  };
+  double* o = out + (size_t)col * n;
+  double* cc = cb + (size_t)col * n;
+  double beta = di(cell(0));
+  double prev = __ddiv_rn(rhs(0), beta);
+  o[0] = prev;
+  for (int j = 1; j < n; ++j) {
+    const size_t c = cell(j), cp = cell(j - 1);
+    const double up = __ddiv_rn(-k[cp * 8 + 6], mu[cp]);
+    const double lo = __ddiv_rn(-k[c * 8 + 2], mu[c]);
+    const double ci = __ddiv_rn(up, beta);
+    cc[j] = ci;
+    beta = __dsub_rn(di(c), __dmul_rn(lo, ci));
+    prev = __ddiv_rn(__dsub_rn(rhs(j), __dmul_rn(lo, prev)), beta);
+    o[j] = prev;
+  }
+  for (int j = n - 2; j >= 0; --j) o[j] = __dsub_rn(o[j], __dmul_rn(cc[j + 1], o[j + 1]));
+}
+
+// x (face row-major) from the column pass's face-column-major result
+__global__ void k_cube_untranspose(int n, const double* __restrict__ t, double* __restrict__ x) {
+  const size_t nn = (size_t)n * n, cells = 6 * nn;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    const size_t f = c / nn, rest = c % nn, j = rest / n, i = rest % n;
+    x[c] = t[f * nn + i * n + j];
+  }
+}
+
+// ---- the V-cycle's levels (multigrid.rs:199-363), FP32 without fused multiply-adds ----
+__global__ void k_mg_val0(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                          const double* __restrict__ mu, const double* __restrict__ diag64, const uint32_t* __restrict__ ptr,
+                          float* __restrict__ val, float* __restrict__ mass, float* __restrict__ diag) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    uint32_t at = ptr[c];
+    for (int s = 0; s < 8; ++s)
+      if (slots[c * 8 + s] != CUBE_NO_CELL) val[at++] = (float)k[c * 8 + s];
+    mass[c] = (float)mu[c];
+    diag[c] = (float)diag64[c];
+  }
+}
+
+__global__ void k_mg_valc(size_t nnz, const uint32_t* __restrict__ src_ptr, const uint32_t* __restrict__ src,
+                          const float* __restrict__ fval, float* __restrict__ cval) {
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nnz; e += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (uint32_t q = src_ptr[e]; q < src_ptr[e + 1]; ++q) s = __fadd_rn(s, fval[src[q]]);
+    cval[e] = __fmul_rn(CUBE_SCALE, s);
+  }
+}
+
+__global__ void k_mg_mass(size_t cells, const uint32_t* __restrict__ kid_ptr, const uint32_t* __restrict__ kids,
+                          const float* __restrict__ fmass, const uint32_t* __restrict__ ptr, const float* __restrict__ val,
+                          float* __restrict__ mass, float* __restrict__ diag) {
+  for (size_t r = blockIdx.x * (size_t)blockDim.x + threadIdx.x; r < cells; r += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (uint32_t q = kid_ptr[r]; q < kid_ptr[r + 1]; ++q) s = __fadd_rn(s, fmass[kids[q]]);
+    float kk = 0.f;
+    for (uint32_t e = ptr[r]; e < ptr[r + 1]; ++e) kk = __fadd_rn(kk, val[e]);
+    mass[r] = s;
+    diag[r] = __fadd_rn(s, kk);
+  }
+}
+
+__device__ __forceinline__ float mg_az(size_t i, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                                       const float* __restrict__ val, const float* __restrict__ diag,
+                                       const float* __restrict__ z) {
+  float az = __fmul_rn(diag[i], z[i]);
+  for (uint32_t e = ptr[i]; e < ptr[i + 1]; ++e) az = __fsub_rn(az, __fmul_rn(val[e], z[col[e]]));
+  return az;
+}
+
+__global__ void k_mg_sweep_first(size_t cells, const float* __restrict__ r, const float* __restrict__ diag, float* __restrict__ z) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x)
+    z[i] = __fdiv_rn(__fmul_rn(CUBE_OMEGA, r[i]), diag[i]);
+}
+
+__global__ void k_mg_sweep(size_t cells, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                           const float* __restrict__ val, const float* __restrict__ diag, const float* __restrict__ r,
+                           const float* __restrict__ z, float* __restrict__ t) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    const float az = mg_az(i, ptr, col, val, diag, z);
+    t[i] = __fadd_rn(z[i], __fdiv_rn(__fmul_rn(CUBE_OMEGA, __fsub_rn(r[i], az)), diag[i]));
+  }
+}
+
+__global__ void k_mg_resid(size_t cells, const uint32_t* __restrict__ ptr, const uint32_t* __restrict__ col,
+                           const float* __restrict__ val, const float* __restrict__ diag, const float* __restrict__ r,
+                           const float* __restrict__ z, float* __restrict__ t) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x)
+    t[i] = __fsub_rn(r[i], mg_az(i, ptr, col, val, diag, z));
+}
+
+__global__ void k_mg_restrict(size_t cells, const uint32_t* __restrict__ kid_ptr, const uint32_t* __restrict__ kids,
+                              const float* __restrict__ t, float* __restrict__ rc) {
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < cells; q += (size_t)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (uint32_t e = kid_ptr[q]; e < kid_ptr[q + 1]; ++e) s = __fadd_rn(s, t[kids[e]]);
+    rc[q] = s;
+  }
+}
+
+__global__ void k_mg_prolong(size_t cells, const uint32_t* __restrict__ parent, const float* __restrict__ zc, float* __restrict__ z) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x)
+    z[c] = __fadd_rn(z[c], zc[parent[c]]);
+}
+
+__global__ void k_to_f32(size_t n, const double* __restrict__ a, float* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (float)a[i];
+}
+__global__ void k_to_f64(size_t n, const float* __restrict__ a, double* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (double)a[i];
+}
+
+// alpha = rz / pap; beta = rz_new / rz, rz = rz_new (the CG scalars, on the device)
+__global__ void k_cube_alpha(const double* __restrict__ rz, const double* __restrict__ pap, double* __restrict__ alpha) {
+  *alpha = *rz / *pap;
+}
+__global__ void k_cube_beta(const double* __restrict__ rz_new, double* __restrict__ rz, double* __restrict__ beta) {
+  *beta = *rz_new / *rz;
+  *rz = *rz_new;
+}
+
+// partials of (rhs - ap) and of s, for the put-back
+__global__ void k_cube_lost(size_t cells, const double* __restrict__ rhs, const double* __restrict__ ap,
+                            const double* __restrict__ s, double* __restrict__ partials) {
+  double a = 0.0, w = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
+    a += rhs[i] - ap[i];
+    w += s[i];
+  }
+  a = block_sum(a);
+  w = block_sum(w);
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = a;
+    partials[CUBE_RED_BLOCKS + blockIdx.x] = w;
+  }
+}
+
+}  // namespace dt
+
+using namespace dt;
+
+namespace {
+
+// One level of the hierarchy: its sparsity (device), its values and vectors.
+struct CubeLevel {
+  size_t cells = 0, nnz = 0, side = 0;
+  uint32_t *ptr = nullptr, *col = nullptr;                      // CSR neighbours
+  uint32_t *src_ptr = nullptr, *src = nullptr;                  // level >= 1: the finer entries summed
+  uint32_t *kid_ptr = nullptr, *kids = nullptr, *parent = nullptr;  // level >= 1: blocks
+  float *val = nullptr, *mass = nullptr, *diag = nullptr, *r = nullptr, *z = nullptr, *t = nullptr;
+};
+
+// The hierarchy's sparsity on the host (multigrid.rs:65-186), built once per grid.
+struct HostPattern {
+  size_t side = 0, cells = 0;
+  std::vector<uint32_t> ptr, col, src_ptr, src, kid_ptr, kids, parent;
+};
+
+HostPattern finest_pattern(size_t n, const uint32_t* slots) {
+  HostPattern p;
+  p.side = n;
+  p.cells = 6 * n * n;
+  p.ptr.push_back(0);
+  for (size_t c = 0; c < p.cells; ++c) {
+    for (int k = 0; k < 8; ++k)
+      if (slots[c * 8 + k] != CUBE_NO_CELL) p.col.push_back(slots[c * 8 + k]);
+    p.ptr.push_back((uint32_t)p.col.size());
+  }
+  return p;
+}
+
+HostPattern coarser_pattern(const HostPattern& f) {
+  const size_t nf = f.side, m = (nf + 1) / 2, cells = 6 * m * m;
+  HostPattern p;
+  p.side = m;
+  p.cells = cells;
+  p.parent.resize(f.cells);
+  for (size_t c = 0; c < f.cells; ++c) {
+    const size_t face = c / (nf * nf), rest = c % (nf * nf), i = rest % nf, j = rest / nf;
+    p.parent[c] = (uint32_t)(face * m * m + (j / 2) * m + i / 2);
+  }
+  p.kid_ptr.assign(cells + 1, 0);
+  for (uint32_t q : p.parent) p.kid_ptr[q + 1] += 1;
+  for (size_t k = 0; k < cells; ++k) p.kid_ptr[k + 1] += p.kid_ptr[k];
+  std::vector<uint32_t> fill(p.kid_ptr.begin(), p.kid_ptr.end() - 1);
+  p.kids.resize(f.cells);
+  for (size_t c = 0; c < f.cells; ++c) p.kids[fill[p.parent[c]]++] = (uint32_t)c;
+  // each coarse cell's neighbours ascending, and per neighbour the fine entries in their order
+  p.ptr.push_back(0);
+  p.src_ptr.push_back(0);
+  std::vector<std::pair<uint32_t, uint32_t>> pairs;
+  for (size_t r = 0; r < cells; ++r) {
+    pairs.clear();
+    for (uint32_t q = p.kid_ptr[r]; q < p.kid_ptr[r + 1]; ++q) {
+      const uint32_t c = p.kids[q];
+      for (uint32_t e = f.ptr[c]; e < f.ptr[c + 1]; ++e) {
+        const uint32_t to = p.parent[f.col[e]];
+        if (to != r) pairs.push_back({to, e});
+      }
+    }
+    std::stable_sort(pairs.begin(), pairs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    for (size_t k = 0; k < pairs.size(); ++k) {
+      if (k == 0 || pairs[k].first != pairs[k - 1].first) {
+        if (k > 0) p.src_ptr.push_back((uint32_t)p.src.size());
+        p.col.push_back(pairs[k].first);
+      }
+      p.src.push_back(pairs[k].second);
+    }
+    if (!pairs.empty()) p.src_ptr.push_back((uint32_t)p.src.size());
+    p.ptr.push_back((uint32_t)p.col.size());
+  }
+  return p;
+}
+
+unsigned int cube_grid(size_t n) { return std::max(1u, std::min<unsigned int>(ceil_div(n, 256), 148u * 8u)); }
+
+}  // namespace
+
+struct dt_cube {
+  int n = 0;
+  size_t cells = 0;
+  double mean_area = 0.0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::vector<void*> allocs;
+  uint32_t* slots = nullptr;
+  double *lap = nullptr, *mu = nullptr;
+  double *kd = nullptr, *h = nullptr;  // staging for the host entry points
+  double *k = nullptr, *s = nullptr, *diag = nullptr;
+  double *rhs = nullptr, *x = nullptr, *b = nullptr, *tmp = nullptr, *cb = nullptr;
+  double *r = nullptr, *z = nullptr, *po = nullptr, *pn = nullptr, *ap = nullptr;
+  double* partials = nullptr;
+  double* sc = nullptr;  // scalars: 0 rr, 1 pap, 2 rz, 3 rz_new, 4 alpha, 5 beta, 6 lost, 7 weight, 8 kk, 9 rhs.rhs
+  std::vector<CubeLevel> levels;
+};
+
+namespace {
+
+template <class T>
+dt_status cube_alloc(dt_cube* s, T** p, size_t count) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("dt_cube: cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? DT_OOM : DT_DEVICE_ERROR;
+  }
+  s->allocs.push_back(q);
+  *p = reinterpret_cast<T*>(q);
+  return DT_OK;
+}
+
+template <class T>
+dt_status cube_upload(dt_cube* s, T** p, const std::vector<T>& v) {
+  DT_TRY(cube_alloc(s, p, v.size()));
+  if (!v.empty()) DT_CUDA(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return DT_OK;
+}
+
+// the sum of n values of partials, in a fixed order, into *out
+void cube_finish(dt_cube* s, const double* partials, double* out) {
+  k_cube_finish<<<1, 1024, 0, s->stream>>>(CUBE_RED_BLOCKS, partials, out);
+}
+
+// K, s, diag for kd and dt (Workspace::build with every cell, diffusion.rs:147-240)
+void cube_build(dt_cube* s, const double* kd, double dt) {
+  k_cube_couplings<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, s->slots, s->lap, kd, s->mu, dt / s->mean_area,
+                                                               s->k, s->s, s->diag);
+}
+
+// the hierarchy's values for the built operator (multigrid.rs:199-269)
+void cube_prepare(dt_cube* s) {
+  CubeLevel& l0 = s->levels[0];
+  k_mg_val0<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, s->slots, s->k, s->mu, s->diag, l0.ptr, l0.val, l0.mass,
+                                                        l0.diag);
+  for (size_t l = 1; l < s->levels.size(); ++l) {
+    CubeLevel &f = s->levels[l - 1], &c = s->levels[l];
+    k_mg_valc<<<cube_grid(c.nnz), 256, 0, s->stream>>>(c.nnz, c.src_ptr, c.src, f.val, c.val);
+    k_mg_mass<<<cube_grid(c.cells), 256, 0, s->stream>>>(c.cells, c.kid_ptr, c.kids, f.mass, c.ptr, c.val, c.mass, c.diag);
+  }
+}
+
+void cube_sweep(dt_cube* s, CubeLevel& lv, bool first) {
+  if (first) {
+    k_mg_sweep_first<<<cube_grid(lv.cells), 256, 0, s->stream>>>(lv.cells, lv.r, lv.diag, lv.z);
+    return;
+  }
+  k_mg_sweep<<<cube_grid(lv.cells), 256, 0, s->stream>>>(lv.cells, lv.ptr, lv.col, lv.val, lv.diag, lv.r, lv.z, lv.t);
+  std::swap(lv.z, lv.t);
+}
+
+// multigrid.rs:312-363
+void cube_vcycle(dt_cube* s, size_t l) {
+  CubeLevel& lv = s->levels[l];
+  if (l + 1 == s->levels.size()) {
+    for (int k = 0; k < CUBE_COARSE_SWEEPS; ++k) cube_sweep(s, lv, k == 0);
+    return;
+  }
+  for (int k = 0; k < CUBE_NU; ++k) cube_sweep(s, lv, k == 0);
+  k_mg_resid<<<cube_grid(lv.cells), 256, 0, s->stream>>>(lv.cells, lv.ptr, lv.col, lv.val, lv.diag, lv.r, lv.z, lv.t);
+  CubeLevel& cl = s->levels[l + 1];
+  k_mg_restrict<<<cube_grid(cl.cells), 256, 0, s->stream>>>(cl.cells, cl.kid_ptr, cl.kids, lv.t, cl.r);
+  cube_vcycle(s, l + 1);
+  k_mg_prolong<<<cube_grid(lv.cells), 256, 0, s->stream>>>(lv.cells, cl.parent, cl.z, lv.z);
+  for (int k = 0; k < CUBE_NU; ++k) cube_sweep(s, lv, false);
+}
+
+// z = V-cycle(r) (multigrid.rs:271-282)
+void cube_precondition(dt_cube* s, const double* r, double* z) {
+  CubeLevel& l0 = s->levels[0];
+  k_to_f32<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, r, l0.r);
+  cube_vcycle(s, 0);
+  k_to_f64<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, l0.z, z);
+}
+
+// the LOD first guess: x from b (diffusion.rs:315-381)
+void cube_lod(dt_cube* s, const double* b, double* x) {
+  const int rows = 6 * s->n;
+  k_cube_lod_rows<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, b, x, s->cb);
+  k_cube_lod_cols<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, x, s->tmp, s->cb);
+  k_cube_untranspose<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->tmp, x);
+}
+
+double read_scalar(dt_cube* s, int i) {
+  double v = 0.0;
+  cudaMemcpyAsync(&v, s->sc + i, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+  cudaStreamSynchronize(s->stream);
+  return v;
+}
+
+// diffusion.rs:270-313 and :387-500 on device arrays h (in/out) and kd
+dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep) {
+  dt_report out{};
+  if (std::isnan(dt) || dt <= 0.0) {
+    if (rep) *rep = out;
+    return DT_OK;
+  }
+  cudaEvent_t e0, e1;
+  DT_CUDA(cudaEventCreate(&e0));
+  DT_CUDA(cudaEventCreate(&e1));
+  DT_CUDA(cudaEventRecord(e0, s->stream));
+  const size_t l = s->cells;
+  const unsigned int G = CUBE_RED_BLOCKS;
+  cube_build(s, kd, dt);
+  k_cube_start<<<cube_grid(l), 256, 0, s->stream>>>(l, h, s->mu, s->rhs, s->x, s->b);
+  cube_lod(s, s->b, s->x);
+  cube_prepare(s);
+  const double tol2 = tol_m * tol_m * (double)l;
+  k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->rhs, s->rhs, s->partials);
+  cube_finish(s, s->partials, s->sc + 9);
+  k_cube_resid<<<G, 256, 0, s->stream>>>(l, s->slots, s->k, s->diag, s->rhs, s->x, s->r, s->partials);
+  cube_finish(s, s->partials, s->sc + 0);
+  double rr = read_scalar(s, 0);
+  int iterations = 0;
+  if (!(rr <= tol2)) {
+    cube_precondition(s, s->r, s->z);
+    k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
+    cube_finish(s, s->partials, s->sc + 2);
+    for (int it = 0; it < CUBE_CG_MAX_ITER; ++it) {
+      k_cube_direction<<<G, 256, 0, s->stream>>>(l, s->slots, s->k, s->diag, s->z, s->po, s->sc + 5, it == 0, s->pn, s->ap,
+                                                 s->partials);
+      cube_finish(s, s->partials, s->sc + 1);
+      std::swap(s->po, s->pn);
+      const double pap = read_scalar(s, 1);
+      if (std::isnan(pap) || pap <= 0.0) break;
+      k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4);
+      k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->po, s->ap, s->x, s->r, s->partials);
+      cube_finish(s, s->partials, s->sc + 0);
+      rr = read_scalar(s, 0);
+      ++iterations;
+      if (rr <= tol2) break;
+      cube_precondition(s, s->r, s->z);
+      k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
+      cube_finish(s, s->partials, s->sc + 3);
+      k_cube_beta<<<1, 1, 0, s->stream>>>(s->sc + 3, s->sc + 2, s->sc + 5);
+    }
+  }
+  // the residual's sum back to the cells, in proportion to their coupling
+  k_cube_apply<<<cube_grid(l), 256, 0, s->stream>>>(l, s->slots, s->k, s->diag, s->x, s->ap);
+  k_cube_lost<<<G, 256, 0, s->stream>>>(l, s->rhs, s->ap, s->s, s->partials);
+  cube_finish(s, s->partials, s->sc + 6);
+  cube_finish(s, s->partials + CUBE_RED_BLOCKS, s->sc + 7);
+  const double lost = read_scalar(s, 6), weight = read_scalar(s, 7);
+  if (weight > 0.0 && lost != 0.0) {
+    const double kk = lost / weight;
+    DT_CUDA(cudaMemcpyAsync(s->sc + 8, &kk, sizeof(double), cudaMemcpyHostToDevice, s->stream));
+    k_cube_putback<<<cube_grid(l), 256, 0, s->stream>>>(l, s->sc + 8, s->s, s->mu, s->x);
+  }
+  DT_CUDA(cudaMemcpyAsync(h, s->x, l * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
+  DT_CUDA(cudaEventRecord(e1, s->stream));
+  DT_CUDA(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  DT_CUDA(cudaGetLastError());
+  out.iterations = iterations;
+  out.converged = rr <= tol2;
+  out.error_m = std::sqrt(rr / (double)l);  // the RMS residual the stop reads, m
+  const double bb = read_scalar(s, 9);
+  out.rel_residual = bb > 0.0 ? std::sqrt(rr / bb) : 0.0;  // ||mu h - A x|| / ||mu h|| before the put-back
+  out.device_ms = ms;
+  if (rep) *rep = out;
+  if (!std::isfinite(rr)) {
+    set_error("dt_cube_diff_solve: the residual is not finite");
+    return DT_NONFINITE;
+  }
+  return out.converged ? DT_OK : DT_NOT_CONVERGED;
+}
+
+}  // namespace
+
+extern "C" {
+
+dt_status dt_cube_destroy(dt_cube* s) {
+  if (!s) return DT_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void* p : s->allocs) cudaFree(p);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return DT_OK;
+}
+
+dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const double* areas, dt_cube** out) {
+  if (!out) {
+    set_error("dt_cube_create: out is NULL");
+    return DT_BAD_ARG;
+  }
+  *out = nullptr;
+  if (n < 2 || n > 8192 || !slots || !lap || !areas) {
+    set_error("dt_cube_create: bad arguments (n %d)", n);
+    return DT_BAD_ARG;
+  }
+  const size_t cells = 6 * (size_t)n * n;
+  for (size_t c = 0; c < cells; ++c) {
+    if (!(areas[c] > 0.0) || !std::isfinite(areas[c])) {
+      set_error("dt_cube_create: area[%zu] is not a positive number", c);
+      return DT_BAD_ARG;
+    }
+    for (int k = 0; k < 8; ++k) {
+      const uint32_t m = slots[c * 8 + k];
+      if ((m != CUBE_NO_CELL && m >= cells) || !std::isfinite(lap[c * 8 + k])) {
+        set_error("dt_cube_create: slot %d of cell %zu is out of range or its weight not finite", k, c);
+        return DT_BAD_ARG;
+      }
+      // only diagonals go missing (a diagonal's coupling reads its two side cells)
+      if ((k & 1) == 0 && m == CUBE_NO_CELL) {
+        set_error("dt_cube_create: side slot %d of cell %zu is empty", k, c);
+        return DT_BAD_ARG;
+      }
+    }
+  }
+  auto* s = new dt_cube();
+  s->n = n;
+  s->cells = cells;
+  auto fail = [&](dt_status e) {
+    dt_cube_destroy(s);
+    return e;
+  };
+  // the mean cell area in the reference's order: per face row, rows in order, faces in order
+  // (sphere/cube.rs:437-449)
+  double total = 0.0;
+  for (int f = 0; f < 6; ++f) {
+    double fs = 0.0;
+    for (int j = 0; j < n; ++j) {
+      double r = 0.0;
+      for (int i = 0; i < n; ++i) r += areas[((size_t)f * n + j) * n + i];
+      fs += r;
+    }
+    total += fs;
+  }
+  s->mean_area = total / (double)cells;
+  std::vector<double> mu(cells);
+  for (size_t c = 0; c < cells; ++c) mu[c] = areas[c] / s->mean_area;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("dt_cube_create: cudaStreamCreate failed");
+    return fail(DT_DEVICE_ERROR);
+  }
+  s->own_stream = true;
+  dt_status st;
+  if ((st = cube_upload(s, &s->slots, std::vector<uint32_t>(slots, slots + cells * 8))) != DT_OK) return fail(st);
+  if ((st = cube_upload(s, &s->lap, std::vector<double>(lap, lap + cells * 8))) != DT_OK) return fail(st);
+  if ((st = cube_upload(s, &s->mu, mu)) != DT_OK) return fail(st);
+  if ((st = cube_alloc(s, &s->k, cells * 8)) != DT_OK) return fail(st);
+  for (double** p : {&s->kd, &s->h, &s->s, &s->diag, &s->rhs, &s->x, &s->b, &s->tmp, &s->cb, &s->r, &s->z, &s->po, &s->pn, &s->ap})
+    if ((st = cube_alloc(s, p, cells)) != DT_OK) return fail(st);
+  if ((st = cube_alloc(s, &s->partials, 2 * CUBE_RED_BLOCKS)) != DT_OK) return fail(st);
+  if ((st = cube_alloc(s, &s->sc, 16)) != DT_OK) return fail(st);
+  // the hierarchy (multigrid.rs:170-186): coarsen while a level has more than 64 cells and a side
+  // above 1
+  std::vector<HostPattern> pats;
+  pats.push_back(finest_pattern(n, slots));
+  while (!(pats.back().cells <= CUBE_COARSEST || pats.back().side <= 1)) pats.push_back(coarser_pattern(pats.back()));
+  s->levels.resize(pats.size());
+  for (size_t l = 0; l < pats.size(); ++l) {
+    const HostPattern& p = pats[l];
+    CubeLevel& lv = s->levels[l];
+    lv.cells = p.cells;
+    lv.nnz = p.col.size();
+    lv.side = p.side;
+    if ((st = cube_upload(s, &lv.ptr, p.ptr)) != DT_OK || (st = cube_upload(s, &lv.col, p.col)) != DT_OK) return fail(st);
+    if (l > 0 && ((st = cube_upload(s, &lv.src_ptr, p.src_ptr)) != DT_OK || (st = cube_upload(s, &lv.src, p.src)) != DT_OK ||
+                  (st = cube_upload(s, &lv.kid_ptr, p.kid_ptr)) != DT_OK || (st = cube_upload(s, &lv.kids, p.kids)) != DT_OK ||
+                  (st = cube_upload(s, &lv.parent, p.parent)) != DT_OK))
+      return fail(st);
+    if ((st = cube_alloc(s, &lv.val, lv.nnz)) != DT_OK) return fail(st);
+    for (float** q : {&lv.mass, &lv.diag, &lv.r, &lv.z, &lv.t})
+      if ((st = cube_alloc(s, q, lv.cells)) != DT_OK) return fail(st);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    set_error("dt_cube_create: %s", cudaGetErrorString(cudaGetLastError()));
+    return fail(DT_DEVICE_ERROR);
+  }
+  *out = s;
+  return DT_OK;
+}
+
+dt_status dt_cube_set_stream(dt_cube* s, void* stream) {
+  if (!s) {
+    set_error("dt_cube_set_stream: NULL handle");
+    return DT_BAD_ARG;
+  }
+  cudaStreamSynchronize(s->stream);
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  s->stream = (cudaStream_t)stream;
+  s->own_stream = false;
+  return DT_OK;
+}
+
+int dt_cube_levels(const dt_cube* s) { return s ? (int)s->levels.size() : -1; }
+
+dt_status dt_cube_diff_solve_dev(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep) {
+  if (!s || !h || !kd || !(tol_m > 0.0)) {
+    set_error("dt_cube_diff_solve_dev: bad arguments");
+    return DT_BAD_ARG;
+  }
+  return cube_solve(s, h, kd, dt, tol_m, rep);
+}
+
+dt_status dt_cube_diff_solve(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep) {
+  if (!s || !h || !kd || !(tol_m > 0.0)) {
+    set_error("dt_cube_diff_solve: bad arguments");
+    return DT_BAD_ARG;
+  }
+  const size_t bytes = s->cells * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->h, h, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, s->stream));
+  dt_status st = cube_solve(s, s->h, s->kd, dt, tol_m, rep);
+  if (st != DT_OK && st != DT_NOT_CONVERGED) return st;
+  DT_CUDA(cudaMemcpyAsync(h, s->h, bytes, cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  return st;
+}
+
+// y = A x for kd and dt (host arrays): the built operator (diffusion.rs:64-86)
+dt_status dt_cube_operator(dt_cube* s, const double* kd, double dt, const double* x, double* y) {
+  if (!s || !kd || !x || !y) {
+    set_error("dt_cube_operator: bad arguments");
+    return DT_BAD_ARG;
+  }
+  const size_t bytes = s->cells * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->h, x, bytes, cudaMemcpyHostToDevice, s->stream));
+  cube_build(s, s->kd, dt);
+  k_cube_apply<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, s->slots, s->k, s->diag, s->h, s->ap);
+  DT_CUDA(cudaMemcpyAsync(y, s->ap, bytes, cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  DT_CUDA(cudaGetLastError());
+  return DT_OK;
+}
+
+// z = V-cycle(r) on the hierarchy of the operator for kd and dt (host arrays)
+dt_status dt_cube_vcycle(dt_cube* s, const double* kd, double dt, const double* r, double* z) {
+  if (!s || !kd || !r || !z) {
+    set_error("dt_cube_vcycle: bad arguments");
+    return DT_BAD_ARG;
+  }
+  const size_t bytes = s->cells * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->r, r, bytes, cudaMemcpyHostToDevice, s->stream));
+  cube_build(s, s->kd, dt);
+  cube_prepare(s);
+  cube_precondition(s, s->r, s->z);
+  DT_CUDA(cudaMemcpyAsync(z, s->z, bytes, cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  DT_CUDA(cudaGetLastError());
+  return DT_OK;
+}
+
+// the LOD first guess x from h for kd and dt (host arrays; diffusion.rs:315-381)
+dt_status dt_cube_lod(dt_cube* s, const double* kd, double dt, const double* h, double* x) {
+  if (!s || !kd || !h || !x) {
+    set_error("dt_cube_lod: bad arguments");
+    return DT_BAD_ARG;
+  }
+  const size_t bytes = s->cells * sizeof(double);
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, s->stream));
+  DT_CUDA(cudaMemcpyAsync(s->b, h, bytes, cudaMemcpyHostToDevice, s->stream));
+  cube_build(s, s->kd, dt);
+  cube_lod(s, s->b, s->x);
+  DT_CUDA(cudaMemcpyAsync(x, s->x, bytes, cudaMemcpyDeviceToHost, s->stream));
+  DT_CUDA(cudaStreamSynchronize(s->stream));
+  DT_CUDA(cudaGetLastError());
+  return DT_OK;
+}
+
+}  // extern "C"

@@ -67,6 +67,14 @@ def lib():
         L.dt_flex_profile_kernels.argtypes = [vp, i, i, vp, vp]
         L.dt_flex_set_unet.argtypes = [vp, vp, d]
         L.dt_flex_operator_dot_noalloc.argtypes = [i, i, d, vp, vp, vp, vp, vp, vp]
+        L.dt_cube_create.argtypes = [i, vp, vp, vp, ctypes.POINTER(vp)]
+        L.dt_cube_destroy.argtypes = [vp]
+        L.dt_cube_set_stream.argtypes = [vp, vp]
+        L.dt_cube_levels.argtypes = [vp]
+        for name in ("dt_cube_diff_solve", "dt_cube_diff_solve_dev"):
+            getattr(L, name).argtypes = [vp, vp, vp, d, d, ctypes.POINTER(Report)]
+        for name in ("dt_cube_operator", "dt_cube_vcycle", "dt_cube_lod"):
+            getattr(L, name).argtypes = [vp, vp, d, vp, vp]
         L.dt_grid_restrict_dev.argtypes = [i, i, i, vp, vp, vp]
         L.dt_grid_prolong_const_dev.argtypes = [i, i, i, vp, vp, vp]
         L.dt_grid_prolong_linear_dev.argtypes = [i, i, i, vp, vp, vp]

@@ -26,6 +26,7 @@
 #ifndef DEEPTIME_GPU_H
 #define DEEPTIME_GPU_H
 #include <stddef.h>
+#include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -200,6 +201,29 @@ dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
  * the bank (its three levels' weighted sum). `precision` selects the FP64 or the FP32 lane. */
 #define DT_PROFILE_KERNELS 10
 dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes);
+
+/* Implicit diffusion on the cube grid (surface/cube/diffusion.rs::solve with
+ * DiffusionSolver::Multigrid, diffusion.rs:244-313): (mu + sum K) x - K x_neighbours = mu h on
+ * the 6 n^2 cells, K = dt / mean_area * D * w per neighbour slot, D the side pair's mean
+ * diffusivity or a diagonal's least quad side mean; the LOD first guess, CG preconditioned by one
+ * FP32 multigrid V-cycle on 2 x 2 face blocks (surface/cube/multigrid.rs), stop at an RMS
+ * residual of tol_m over every cell or after 400 iterations, then the residual's sum put back so
+ * that sum(area h) is kept. The grid's geometry comes from the caller's CubeGrid at create:
+ * slots (6 n^2 x 8, CubeTopology::slots in OFFSETS order, 0xFFFFFFFF where there is none), lap
+ * (6 n^2 x 8, CubeGrid::lap) and areas (6 n^2, CubeGrid::areas). The report's error_m is the
+ * final RMS residual (m), rel_residual ||mu h - A x|| / ||mu h||. Status DT_NOT_CONVERGED after
+ * 400 iterations (h still holds the last iterate, as the reference leaves it). */
+typedef struct dt_cube dt_cube;
+dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const double* areas, dt_cube** out);
+dt_status dt_cube_destroy(dt_cube* s);
+dt_status dt_cube_set_stream(dt_cube* s, void* stream);
+int dt_cube_levels(const dt_cube* s); /* the V-cycle's levels, -1 for NULL */
+dt_status dt_cube_diff_solve(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep);
+dt_status dt_cube_diff_solve_dev(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep);
+/* host arrays: y = A x of the operator for kd and dt; z = one V-cycle of r; the LOD first guess */
+dt_status dt_cube_operator(dt_cube* s, const double* kd, double dt, const double* x, double* y);
+dt_status dt_cube_vcycle(dt_cube* s, const double* kd, double dt, const double* r, double* z);
+dt_status dt_cube_lod(dt_cube* s, const double* kd, double dt, const double* h, double* x);
 
 /* The flexure step's grid helpers on device arrays (row-major, x fastest), enqueued on `stream`
  * (NULL: the legacy default stream) without a host sync; each result is bit-for-bit the

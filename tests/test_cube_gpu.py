@@ -1,0 +1,73 @@
+"""The cube grid's diffusion solve on the device (dt_cube_*) against the oracle's restatement of
+the reference (surface/cube/diffusion.rs, surface/cube/multigrid.rs), through the C ABI.
+
+Tolerances: the operator and the LOD first guess are FP64 with the reference's operation order,
+compared at 1e-14 relative; the V-cycle is FP32, compared at 1e-6 relative; solves stop at an RMS
+residual of tol, so the two answers are compared at 100 tol (m) absolute, their iteration counts
+within one, and the volume sum(mu h) to 1e-9 relative."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from deeptime_gpu import cube as C
+from tests.fixtures import cube_case
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module", params=[8, 13, 32])
+def case(request):
+    n = request.param
+    slots = O.cube_topology(n)
+    lap, areas, kd, h = cube_case(n, n + 100, slots)
+    return n, slots, lap, areas, kd, h, C.CubeDiffusion(n, slots, lap, areas)
+
+
+def test_operator_matches_the_oracle(case):
+    n, slots, lap, areas, kd, h, dev = case
+    x = np.random.default_rng(1).standard_normal(6 * n * n)
+    assert rel(dev.operator(kd, 7.0, x), O.cube_operator(n, slots, lap, areas, kd, 7.0, x)) < 1e-14
+
+
+def test_lod_first_guess_matches_the_oracle(case):
+    n, slots, lap, areas, kd, h, dev = case
+    assert rel(dev.lod(kd, 7.0, h), O.cube_lod(n, slots, lap, areas, kd, 7.0, h)) < 1e-14
+
+
+def test_vcycle_matches_the_oracle(case):
+    n, slots, lap, areas, kd, h, dev = case
+    r = np.random.default_rng(2).standard_normal(6 * n * n)
+    assert rel(dev.vcycle(kd, 7.0, r), O.cube_vcycle(n, slots, lap, areas, kd, 7.0, r)) < 1e-6
+
+
+@pytest.mark.parametrize("dt", [0.5, 7.0, 60.0])
+def test_solve_matches_the_oracle_and_keeps_the_volume(case, dt):
+    n, slots, lap, areas, kd, h, dev = case
+    tol = 1e-6
+    want, its = O.cube_diff_solve(n, slots, lap, areas, kd, dt, tol, h)
+    got, rep = dev.solve(h, kd, dt, tol)
+    assert rep.converged and rep.error_m <= tol
+    assert abs(rep.iterations - its) <= 1, (rep.iterations, its)
+    assert np.abs(got - want).max() < 100 * tol
+    mu = areas / (areas.sum() / areas.size)
+    assert abs((mu * got).sum() - (mu * h).sum()) <= 1e-9 * np.abs(mu * h).sum()
+
+
+def test_no_step_leaves_the_field_as_it_was(case):
+    n, slots, lap, areas, kd, h, dev = case
+    for dt in (0.0, float("nan")):
+        got, rep = dev.solve(h, kd, dt, 1e-6)
+        assert rep.iterations == 0 and np.array_equal(got, h)
+
+
+def test_the_hierarchy_reaches_64_cells():
+    n = 32
+    slots = O.cube_topology(n)
+    lap, areas, kd, h = cube_case(n, 1, slots)
+    dev = C.CubeDiffusion(n, slots, lap, areas)
+    # sides 32, 16, 8, 4, 2: the last level 24 cells (the first at or below 64)
+    assert dev.levels == 5
