@@ -74,19 +74,13 @@ def cube_case(n, seed, slots):
     rng = np.random.default_rng(seed)
     cells = 6 * n * n
     areas = 1.0 + 0.2 * rng.random(cells)
-    lap = np.zeros((cells, 8))
     raw = np.where(np.arange(8) % 2 == 0, 0.8 + 0.4 * rng.random((cells, 8)), 0.05 + 0.15 * rng.random((cells, 8)))
-    none = slots == 0xFFFFFFFF
-    for c in range(cells):
-        for k in range(8):
-            m = int(slots[c, k])
-            if none[c, k]:
-                continue
-            if m > c:
-                lap[c, k] = raw[c, k]
-            else:
-                km = int(np.nonzero(slots[m] == c)[0][0])
-                lap[c, k] = raw[m, km]
+    valid = slots != 0xFFFFFFFF
+    m = np.where(valid, slots, 0).astype(np.int64)
+    c = np.arange(cells)[:, None]
+    km = np.argmax(slots[m] == c[:, :, None], axis=2)  # the slot of c in its neighbour m's table
+    lap = np.where(m > c, raw, raw[m, km])
+    lap = np.where(valid, lap, 0.0)
     kd = np.where(rng.random(cells) < 0.3, 0.02, 1.0) * (0.5 + rng.random(cells))
     h = 1000.0 * rng.standard_normal(cells)
     return lap, areas, kd, h
