@@ -78,3 +78,16 @@ def test_bad_arguments_are_refused():
     assert lib.dt_grid_prolong_linear_dev(0, 4, 2, ptr(t), ptr(t), None) == L.DT_BAD_ARG
     assert lib.dt_grid_binomial_dev(4, 4, 1, ptr(t), None, None) == L.DT_BAD_ARG
     assert lib.dt_grid_box_blur_dev(4, 4, 1, -1, 1, ptr(t), ptr(t), None) == L.DT_BAD_ARG
+
+
+def test_the_python_mirror_runs_the_same_kernels():
+    from deeptime_gpu import grid as Gr
+
+    rng = np.random.default_rng(9)
+    v = rng.standard_normal((64, 96)) * 10.0
+    c = Gr.restrict(dev(v), 4)
+    assert np.array_equal(host(c), O.restrict_by(v, 4))
+    assert np.array_equal(host(Gr.prolong_linear(c, 4)), O.prolong_linear(O.restrict_by(v, 4), 4))
+    assert np.array_equal(host(Gr.prolong_const(c, 4)), O.prolong_const(O.restrict_by(v, 4), 4))
+    assert np.array_equal(host(Gr.binomial(dev(v), 2)), O.binomial(v, 2))
+    assert np.array_equal(host(Gr.box_blur(dev(v), 2, 2, wrap_x=False)), O.box_blur(v, 2, 2, wrap=False))
