@@ -568,12 +568,24 @@ void cube_lod(dt_cube* s, const double* b, double* x) {
   k_cube_untranspose<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->tmp, x);
 }
 
+// One device scalar to the host (a sync); a device error reads as NaN, which ends the loop and
+// is reported as DT_NONFINITE or by the final error check.
 double read_scalar(dt_cube* s, int i) {
   double v = 0.0;
-  cudaMemcpyAsync(&v, s->sc + i, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
-  cudaStreamSynchronize(s->stream);
+  if (cudaMemcpyAsync(&v, s->sc + i, sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return std::nan("");
   return v;
 }
+
+// The solve's two timing events, destroyed on every way out.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
 
 // diffusion.rs:270-313 and :387-500 on device arrays h (in/out) and kd
 dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double tol_m, dt_report* rep) {
@@ -582,10 +594,10 @@ dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double 
     if (rep) *rep = out;
     return DT_OK;
   }
-  cudaEvent_t e0, e1;
-  DT_CUDA(cudaEventCreate(&e0));
-  DT_CUDA(cudaEventCreate(&e1));
-  DT_CUDA(cudaEventRecord(e0, s->stream));
+  EventPair ev;
+  DT_CUDA(cudaEventCreate(&ev.a));
+  DT_CUDA(cudaEventCreate(&ev.b));
+  DT_CUDA(cudaEventRecord(ev.a, s->stream));
   const size_t l = s->cells;
   const unsigned int G = CUBE_RED_BLOCKS;
   cube_build(s, kd, dt);
@@ -634,12 +646,10 @@ dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double 
     k_cube_putback<<<cube_grid(l), 256, 0, s->stream>>>(l, s->sc + 8, s->s, s->mu, s->x);
   }
   DT_CUDA(cudaMemcpyAsync(h, s->x, l * sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
-  DT_CUDA(cudaEventRecord(e1, s->stream));
-  DT_CUDA(cudaEventSynchronize(e1));
+  DT_CUDA(cudaEventRecord(ev.b, s->stream));
+  DT_CUDA(cudaEventSynchronize(ev.b));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaEventElapsedTime(&ms, ev.a, ev.b);
   DT_CUDA(cudaGetLastError());
   out.iterations = iterations;
   out.converged = rr <= tol2;
