@@ -160,9 +160,10 @@ __global__ void k_cube_direction(size_t cells, const uint32_t* __restrict__ slot
 }
 
 // x += alpha p; r -= alpha A p; partial r.r (diffusion.rs:448-475)
-__global__ void k_cube_update(size_t cells, const double* __restrict__ alpha_p, const double* __restrict__ p,
-                              const double* __restrict__ ap, double* __restrict__ x, double* __restrict__ r,
-                              double* __restrict__ partials) {
+__global__ void k_cube_update(size_t cells, const double* __restrict__ alpha_p, const double* __restrict__ broke,
+                              const double* __restrict__ p, const double* __restrict__ ap, double* __restrict__ x,
+                              double* __restrict__ r, double* __restrict__ partials) {
+  if (*broke != 0.0) return;  // the loop stops before the update
   const double alpha = *alpha_p;
   double acc = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
@@ -359,8 +360,16 @@ __global__ void k_to_f64(size_t n, const float* __restrict__ a, double* __restri
 }
 
 // alpha = rz / pap; beta = rz_new / rz, rz = rz_new (the CG scalars, on the device)
-__global__ void k_cube_alpha(const double* __restrict__ rz, const double* __restrict__ pap, double* __restrict__ alpha) {
-  *alpha = *rz / *pap;
+// alpha = rz / pap, or the breakdown flag (pap not positive, or NaN: diffusion.rs:444-446)
+__global__ void k_cube_alpha(const double* __restrict__ rz, const double* __restrict__ pap, double* __restrict__ alpha,
+                             double* __restrict__ broke) {
+  const double p = *pap;
+  if (isnan(p) || p <= 0.0) {
+    *broke = 1.0;
+  } else {
+    *broke = 0.0;
+    *alpha = *rz / p;
+  }
 }
 __global__ void k_cube_beta(const double* __restrict__ rz_new, double* __restrict__ rz, double* __restrict__ beta) {
   *beta = *rz_new / *rz;
@@ -478,8 +487,14 @@ struct dt_cube {
   double *rhs = nullptr, *x = nullptr, *b = nullptr, *tmp = nullptr, *cb = nullptr;
   double *r = nullptr, *z = nullptr, *po = nullptr, *pn = nullptr, *ap = nullptr;
   double* partials = nullptr;
-  double* sc = nullptr;  // scalars: 0 rr, 1 pap, 2 rz, 3 rz_new, 4 alpha, 5 beta, 6 lost, 7 weight, 8 kk, 9 rhs.rhs
+  double* sc = nullptr;  // scalars: 0 rr, 1 pap, 2 rz, 3 rz_new, 4 alpha, 5 beta, 6 lost, 7 weight, 8 kk, 9 rhs.rhs,
+                        // 10 breakdown flag, 11 the update's r.r
   std::vector<CubeLevel> levels;
+  // The V-cycle's launches as CUDA graphs. Every level swaps its sweep buffers an odd number of
+  // times a cycle, so the buffers alternate between two layouts: one graph for each, captured on
+  // first use.
+  cudaGraphExec_t vcycle_exec[2] = {nullptr, nullptr};
+  int vcycle_layout = 0;
 };
 
 namespace {
@@ -553,11 +568,38 @@ void cube_vcycle(dt_cube* s, size_t l) {
 }
 
 // z = V-cycle(r) (multigrid.rs:271-282)
-void cube_precondition(dt_cube* s, const double* r, double* z) {
+void cube_precondition_launches(dt_cube* s, const double* r, double* z) {
   CubeLevel& l0 = s->levels[0];
   k_to_f32<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, r, l0.r);
   cube_vcycle(s, 0);
   k_to_f64<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->cells, l0.z, z);
+}
+
+// z = V-cycle(r) for the handle's r and z, through the graph of the current buffer layout
+// (captured the first time; capturing runs the host side of the cycle, which leaves the layout
+// flipped as the graph's run does)
+dt_status cube_precondition(dt_cube* s) {
+  const int lay = s->vcycle_layout;
+  if (!s->vcycle_exec[lay]) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      // a stream that cannot be captured (the legacy default stream): the launches themselves
+      cudaGetLastError();
+      cube_precondition_launches(s, s->r, s->z);
+      s->vcycle_layout ^= 1;
+      return DT_OK;
+    }
+    cube_precondition_launches(s, s->r, s->z);
+    DT_CUDA(cudaStreamEndCapture(s->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&s->vcycle_exec[lay], g, 0);
+    cudaGraphDestroy(g);
+    DT_CUDA(e);
+  } else {
+    for (CubeLevel& lv : s->levels) std::swap(lv.z, lv.t);  // the layout the run leaves
+  }
+  DT_CUDA(cudaGraphLaunch(s->vcycle_exec[lay], s->stream));
+  s->vcycle_layout ^= 1;
+  return DT_OK;
 }
 
 // the LOD first guess: x from b (diffusion.rs:315-381)
@@ -612,7 +654,7 @@ dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double 
   double rr = read_scalar(s, 0);
   int iterations = 0;
   if (!(rr <= tol2)) {
-    cube_precondition(s, s->r, s->z);
+    DT_TRY(cube_precondition(s));
     k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
     cube_finish(s, s->partials, s->sc + 2);
     for (int it = 0; it < CUBE_CG_MAX_ITER; ++it) {
@@ -620,15 +662,23 @@ dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double 
                                                  s->partials);
       cube_finish(s, s->partials, s->sc + 1);
       std::swap(s->po, s->pn);
-      const double pap = read_scalar(s, 1);
-      if (std::isnan(pap) || pap <= 0.0) break;
-      k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4);
-      k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->po, s->ap, s->x, s->r, s->partials);
-      cube_finish(s, s->partials, s->sc + 0);
-      rr = read_scalar(s, 0);
+      k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4, s->sc + 10);
+      k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->sc + 10, s->po, s->ap, s->x, s->r, s->partials);
+      cube_finish(s, s->partials, s->sc + 11);
+      // one read back an iteration: the new r.r and the breakdown flag
+      double back[2] = {std::nan(""), 1.0};
+      if (cudaMemcpyAsync(back, s->sc + 10, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+          cudaStreamSynchronize(s->stream) != cudaSuccess)
+        back[0] = 1.0, back[1] = std::nan("");
+      if (back[0] != 0.0) {  // pap <= 0 or NaN (or a failed read): no update
+        if (std::isnan(back[1])) rr = back[1];
+        break;
+      }
+      rr = back[1];
+      DT_CUDA(cudaMemcpyAsync(s->sc + 0, s->sc + 11, sizeof(double), cudaMemcpyDeviceToDevice, s->stream));
       ++iterations;
       if (rr <= tol2) break;
-      cube_precondition(s, s->r, s->z);
+      DT_TRY(cube_precondition(s));
       k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
       cube_finish(s, s->partials, s->sc + 3);
       k_cube_beta<<<1, 1, 0, s->stream>>>(s->sc + 3, s->sc + 2, s->sc + 5);
@@ -672,6 +722,8 @@ extern "C" {
 dt_status dt_cube_destroy(dt_cube* s) {
   if (!s) return DT_OK;
   if (s->stream) cudaStreamSynchronize(s->stream);
+  for (cudaGraphExec_t& e : s->vcycle_exec)
+    if (e) cudaGraphExecDestroy(e);
   for (void* p : s->allocs) cudaFree(p);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -837,7 +889,7 @@ dt_status dt_cube_vcycle(dt_cube* s, const double* kd, double dt, const double* 
   DT_CUDA(cudaMemcpyAsync(s->r, r, bytes, cudaMemcpyHostToDevice, s->stream));
   cube_build(s, s->kd, dt);
   cube_prepare(s);
-  cube_precondition(s, s->r, s->z);
+  DT_TRY(cube_precondition(s));
   DT_CUDA(cudaMemcpyAsync(z, s->z, bytes, cudaMemcpyDeviceToHost, s->stream));
   DT_CUDA(cudaStreamSynchronize(s->stream));
   DT_CUDA(cudaGetLastError());

@@ -46,12 +46,21 @@ struct LevelBufs {
   int cu;          // channels of U
 };
 
+// A pixel's UNET_IN_PAD channels are UNET_IN_PAD / 8 words of 16 bytes; consecutive threads write
+// consecutive words (the first of a pixel holds its two input channels, the rest zeros).
 __global__ void k_pack_input(size_t npix, const float* __restrict__ x, bf16* __restrict__ out) {
-  for (size_t p = blockIdx.x * (size_t)blockDim.x + threadIdx.x; p < npix; p += (size_t)gridDim.x * blockDim.x) {
-    bf16* o = out + p * UNET_IN_PAD;
-    o[0] = __float2bfloat16(x[2 * p]);
-    o[1] = __float2bfloat16(x[2 * p + 1]);
-    for (int c = 2; c < UNET_IN_PAD; ++c) o[c] = __float2bfloat16(0.f);
+  constexpr int WPP = UNET_IN_PAD / 8;
+  static_assert(WPP * 8 == UNET_IN_PAD && (WPP & (WPP - 1)) == 0, "whole 16-byte words per pixel");
+  uint4* o = reinterpret_cast<uint4*>(out);
+  const size_t nw = npix * WPP;
+  for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < nw; q += (size_t)gridDim.x * blockDim.x) {
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if ((q & (WPP - 1)) == 0) {
+      const size_t p = q / WPP;
+      __nv_bfloat162 b = __floats2bfloat162_rn(x[2 * p], x[2 * p + 1]);
+      v.x = *reinterpret_cast<const unsigned int*>(&b);
+    }
+    o[q] = v;
   }
 }
 
@@ -668,7 +677,7 @@ dt_status unet_predict_on(dt_unet* u, cudaStream_t st, const float* x, float* y,
   DT_TRY(unet_check_shape(B, H, W));
   DT_TRY(unet_batch(u, B, H, W));
   size_t npix = (size_t)B * H * W;
-  k_pack_input<<<ugrid(u, npix), 256, 0, st>>>(npix, x, u->X0);
+  k_pack_input<<<ugrid(u, npix * (UNET_IN_PAD / 8)), 256, 0, st>>>(npix, x, u->X0);
   count_launch();
   unet_forward(u, st);
   DT_CUDA(cudaMemcpyAsync(y, u->pred, npix * sizeof(float), cudaMemcpyDeviceToDevice, st));
@@ -766,7 +775,7 @@ dt_status dt_unet_train_step_dev(dt_unet* u, const float* x, const float* t, int
   DT_TRY(unet_batch(u, B, H, W));
   cudaStream_t st = u->stream;
   size_t npix = (size_t)B * H * W;
-  k_pack_input<<<ugrid(u, npix), 256, 0, st>>>(npix, x, u->X0);
+  k_pack_input<<<ugrid(u, npix * (UNET_IN_PAD / 8)), 256, 0, st>>>(npix, x, u->X0);
   count_launch();
   unet_forward(u, st);
   unsigned int lg = std::min<unsigned int>(ceil_div(npix, 256), (unsigned)u->sms * 16);
@@ -817,7 +826,7 @@ dt_status dt_unet_loss_and_grad_dev(dt_unet* u, const float* x, const float* t, 
   DT_TRY(unet_batch(u, B, H, W));
   cudaStream_t st = u->stream;
   size_t npix = (size_t)B * H * W;
-  k_pack_input<<<ugrid(u, npix), 256, 0, st>>>(npix, x, u->X0);
+  k_pack_input<<<ugrid(u, npix * (UNET_IN_PAD / 8)), 256, 0, st>>>(npix, x, u->X0);
   unet_forward(u, st);
   unsigned int lg = std::min<unsigned int>(ceil_div(npix, 256), (unsigned)u->sms * 16);
   k_mse<<<lg, 256, 0, st>>>(npix, u->pred, t, u->dpred, u->loss_part);

@@ -71,3 +71,11 @@ def test_the_hierarchy_reaches_64_cells():
     dev = C.CubeDiffusion(n, slots, lap, areas)
     # sides 32, 16, 8, 4, 2: the last level 24 cells (the first at or below 64)
     assert dev.levels == 5
+
+
+def test_a_level_field_stays_level_on_the_device(case):
+    n, slots, lap, areas, kd, h, dev = case
+    level = np.full(6 * n * n, -42.5)
+    got, rep = dev.solve(level, kd, 30.0, 1e-6)
+    assert rep.iterations == 0
+    assert np.allclose(got, level, rtol=1e-12, atol=0)

@@ -84,3 +84,14 @@ def test_the_first_guess_is_a_smoothing_of_the_field():
     # no coupling: the first guess is the field itself
     x0 = O.cube_lod(n, s, lap, areas, np.zeros_like(kd), 4.0, h)
     assert np.array_equal(x0, h)
+
+
+def test_a_level_field_stays_level():
+    # A constant h is its own implicit step: A h = mu h, so the LOD guess returns it and CG stops at once
+    n = 10
+    s = O.cube_topology(n)
+    lap, areas, kd, _ = cube_case(n, 11, s)
+    h = np.full(6 * n * n, 123.25)
+    x, its = O.cube_diff_solve(n, s, lap, areas, kd, 30.0, 1e-6, h)
+    assert its == 0
+    assert np.allclose(x, h, rtol=1e-12, atol=0)
