@@ -166,8 +166,15 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
     int j = t & (NBF - 1);
     C* base = s + b * NP;
     int k = j & (NS - 1);
+    if constexpr (NBF % 16 == 0) {
+      // j < NBF: pad(j + r NBF) = pad(j) + r (NBF + NBF / 16), constant offsets from one base
+      const C* bj = base + Pad<C>::at(j);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q][r] = base[Pad<C>::at(j + r * NBF)];
+      for (int r = 0; r < R; ++r) v[q][r] = bj[r * (NBF + NBF / 16)];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q][r] = base[Pad<C>::at(j + r * NBF)];
+    }
     if (NS > 1) {
       C w[R];
       stage_twiddles<C, R, INV>(tw, STEP * k, w);
@@ -181,8 +188,20 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
 #pragma unroll
   for (int q = 0; q < B; ++q) {
     dft_r<C, R, INV>(v[q]);
+    if constexpr (NS % 16 == 0) {
+      // oidx + r NS with NS a multiple of 16: pad(oidx) + r (NS + NS / 16)
+      C* o = s + obase[q] + Pad<C>::at(oidx[q]);
 #pragma unroll
-    for (int r = 0; r < R; ++r) s[obase[q] + Pad<C>::at(oidx[q] + r * NS)] = v[q][r];
+      for (int r = 0; r < R; ++r) o[r * (NS + NS / 16)] = v[q][r];
+    } else if constexpr (NS == 1) {
+      // oidx = j R with R <= 16 and r < R: the 16-slot group does not change, pad(oidx) + r
+      C* o = s + obase[q] + Pad<C>::at(oidx[q]);
+#pragma unroll
+      for (int r = 0; r < R; ++r) o[r] = v[q][r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[obase[q] + Pad<C>::at(oidx[q] + r * NS)] = v[q][r];
+    }
   }
   __syncthreads();
 }

@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
     }
     dft_r<C, 16, false>(z);
 #pragma unroll
-    for (int r = 0; r < 16; ++r) s[P::at(j * 16 + r)] = z[r];
+    for (int r = 0; r < 16; ++r) s[17 * j + r] = z[r];  // pad(16 j + r) = 17 j + r
     __syncthreads();
     Stages<C, FFT_EPT, false, LOGN, 16, LOGN - 4>::run(s, tw);
   } else {
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
     dft_r<C, 16, false>(v);
     C* col = s + cc * HP;
 #pragma unroll
-    for (int r = 0; r < 16; ++r) col[P::at(j * 16 + r)] = v[r];
+    for (int r = 0; r < 16; ++r) col[17 * j + r] = v[r];  // pad(16 j + r) = 17 j + r
     __syncthreads();
     Stages<C, FFT_EPT, false, LOGH, 16, LOGH - 4, HP>::run(s, tw);
   }
@@ -968,7 +968,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
       const C* col = s + cc * HP;
       C v[RL];
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[r] = col[P::at(j + r * NSL)];
+      for (int r = 0; r < RL; ++r) v[r] = col[P::at(j) + r * (NSL + NSL / 16)];  // j < NSL, a multiple of 16
       if (NSL > 1) {
         C w[RL];
         stage_twiddles<C, RL, true>(tw_inv, j, w);
@@ -1233,7 +1233,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       const int j = tid + q * NT;
       C z[RL];
 #pragma unroll
-      for (int rr = 0; rr < RL; ++rr) z[rr] = s[P::at(j + rr * NSL)];
+      for (int rr = 0; rr < RL; ++rr) z[rr] = s[P::at(j) + rr * (NSL + NSL / 16)];  // j < NSL, a multiple of 16
       if (NSL > 1) {
         C wv[RL];
         stage_twiddles<C, RL, true>(tw, j, wv);
