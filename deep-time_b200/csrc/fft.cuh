@@ -148,7 +148,7 @@ __device__ __forceinline__ void dft_r(C* v) {
 // One stage of radix R over the block's sequences of length N = 2^LOGN, each stored at
 // s + b * NP (padded); span NS. Everything but the data is known at compile time, so the index
 // arithmetic is shifts and masks. Threads: batch * N / EPT, each owns EPT / R butterflies.
-template <class C, int R, int EPT, bool INV, int LOGN, int NS, int PITCH = 0>
+template <class C, int R, int EPT, bool INV, int LOGN, int NS, int PITCH = 0, int NTH = 0>
 __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   constexpr int N = 1 << LOGN;
   constexpr int NP = PITCH ? PITCH : Pad<C>::len(N);
@@ -161,7 +161,9 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
   int obase[B], oidx[B];
 #pragma unroll
   for (int q = 0; q < B; ++q) {
-    int t = tid + q * blockDim.x;
+    // NTH: the block's threads when the caller knows them at compile time (index arithmetic
+    // folds), else blockDim.x
+    int t = tid + q * (NTH ? NTH : (int)blockDim.x);
     int b = t >> LOGNBF;
     int j = t & (NBF - 1);
     C* base = s + b * NP;
@@ -208,19 +210,19 @@ __device__ __forceinline__ void stockham_stage(C* s, const C* __restrict__ tw) {
 
 // Stages from span NS on: radix 16 while four or more factors of two remain (and a thread holds
 // 16 values), then 8, 4 or 2.
-template <class C, int EPT, bool INV, int LOGN, int NS, int REM, int PITCH = 0>
+template <class C, int EPT, bool INV, int LOGN, int NS, int REM, int PITCH = 0, int NTH = 0>
 struct Stages {
   static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
     if constexpr (REM >= 4 && EPT % 16 == 0) {
-      stockham_stage<C, 16, EPT, INV, LOGN, NS, PITCH>(s, tw);
-      Stages<C, EPT, INV, LOGN, NS * 16, REM - 4, PITCH>::run(s, tw);
+      stockham_stage<C, 16, EPT, INV, LOGN, NS, PITCH, NTH>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 16, REM - 4, PITCH, NTH>::run(s, tw);
     } else if constexpr (REM >= 3) {
-      stockham_stage<C, 8, EPT, INV, LOGN, NS, PITCH>(s, tw);
-      Stages<C, EPT, INV, LOGN, NS * 8, REM - 3, PITCH>::run(s, tw);
+      stockham_stage<C, 8, EPT, INV, LOGN, NS, PITCH, NTH>(s, tw);
+      Stages<C, EPT, INV, LOGN, NS * 8, REM - 3, PITCH, NTH>::run(s, tw);
     } else if constexpr (REM == 2) {
-      stockham_stage<C, 4, EPT, INV, LOGN, NS, PITCH>(s, tw);
+      stockham_stage<C, 4, EPT, INV, LOGN, NS, PITCH, NTH>(s, tw);
     } else if constexpr (REM == 1) {
-      stockham_stage<C, 2, EPT, INV, LOGN, NS, PITCH>(s, tw);
+      stockham_stage<C, 2, EPT, INV, LOGN, NS, PITCH, NTH>(s, tw);
     }
   }
 };
@@ -232,9 +234,9 @@ __host__ __device__ constexpr int last_radix(int logn) {
 
 // Full transform of length 2^LOGN. The caller synchronises before (data in s) and may read s
 // after it returns.
-template <class C, int EPT, bool INV, int LOGN>
+template <class C, int EPT, bool INV, int LOGN, int NTH = 0>
 __device__ __forceinline__ void smem_fft(C* s, const C* __restrict__ tw) {
-  Stages<C, EPT, INV, LOGN, 1, LOGN>::run(s, tw);
+  Stages<C, EPT, INV, LOGN, 1, LOGN, 0, NTH>::run(s, tw);
 }
 
 }  // namespace dt

@@ -768,7 +768,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
 #pragma unroll
     for (int r = 0; r < 16; ++r) s[17 * j + r] = z[r];  // pad(16 j + r) = 17 j + r
     __syncthreads();
-    Stages<C, FFT_EPT, false, LOGN, 16, LOGN - 4>::run(s, tw);
+    Stages<C, FFT_EPT, false, LOGN, 16, LOGN - 4, 0, NT>::run(s, tw);
   } else {
 #pragma unroll 1
     for (int q0 = 0; q0 < FFT_EPT; q0 += FFT_BATCH) {
@@ -797,7 +797,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       }
     }
     __syncthreads();
-    smem_fft<C, FFT_EPT, false, LOGN>(s, tw);
+    smem_fft<C, FFT_EPT, false, LOGN, NT>(s, tw);
   }
   // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
   constexpr int half_n = N / 2 + 1;
@@ -865,7 +865,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
       }
     }
     __syncthreads();
-    Stages<C, FFT_EPT, false, LOGH, 1, LOGH, HP>::run(s, tw);
+    Stages<C, FFT_EPT, false, LOGH, 1, LOGH, HP, NT>::run(s, tw);
   } else {
     // The forward transform's first stage (radix 16, span 1) straight from global memory: thread
     // tid takes butterfly j = tid / CPB of column tid % CPB, i.e. v[j + r h/16], r = 0 .. 15; a
@@ -880,7 +880,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
 #pragma unroll
     for (int r = 0; r < 16; ++r) col[17 * j + r] = v[r];  // pad(16 j + r) = 17 j + r
     __syncthreads();
-    Stages<C, FFT_EPT, false, LOGH, 16, LOGH - 4, HP>::run(s, tw);
+    Stages<C, FFT_EPT, false, LOGH, 16, LOGH - 4, HP, NT>::run(s, tw);
   }
   // per column and pair (m, h - m): C[m] = (w_m V[m] + i w_(h-m) V[h-m]) / 2, divide, and back
   constexpr int half_h = h / 2 + 1;
@@ -944,7 +944,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   asm volatile("mov.b64 %0, %1;" : "=l"(tw_inv) : "l"(tw));
   const T inv_h = (T)1 / (T)h;
   if constexpr (LOGH < 4) {
-    Stages<C, FFT_EPT, true, LOGH, 1, LOGH, HP>::run(s, tw_inv);
+    Stages<C, FFT_EPT, true, LOGH, 1, LOGH, HP, NT>::run(s, tw_inv);
 #pragma unroll 4
     for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
       int j = idx >> logc, cc = idx & (CPB - 1);
@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
     constexpr int RL = last_radix(LOGH);
     constexpr int LOGRL = RL == 16 ? 4 : RL == 8 ? 3 : RL == 4 ? 2 : 1;
     constexpr int NSL = h / RL;
-    Stages<C, FFT_EPT, true, LOGH, 1, LOGH - LOGRL, HP>::run(s, tw_inv);
+    Stages<C, FFT_EPT, true, LOGH, 1, LOGH - LOGRL, HP, NT>::run(s, tw_inv);
 #pragma unroll
     for (int q = 0; q < FFT_EPT / RL; ++q) {
       const int u = tid + q * NT;
@@ -1227,7 +1227,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
     constexpr int RL = last_radix(LOGN);
     constexpr int LOGRL = RL == 16 ? 4 : RL == 8 ? 3 : RL == 4 ? 2 : 1;
     constexpr int NSL = N / RL;
-    Stages<C, FFT_EPT, true, LOGN, 1, LOGN - LOGRL>::run(s, tw);
+    Stages<C, FFT_EPT, true, LOGN, 1, LOGN - LOGRL, 0, NT>::run(s, tw);
 #pragma unroll
     for (int q = 0; q < FFT_EPT / RL; ++q) {
       const int j = tid + q * NT;
@@ -1247,7 +1247,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
       }
     }
   } else {
-    smem_fft<C, FFT_EPT, true, LOGN>(s, tw);
+    smem_fft<C, FFT_EPT, true, LOGN, NT>(s, tw);
 #pragma unroll 4
     for (int idx = tid; idx < RB * N; idx += blockDim.x) {
       int rb = idx >> logN, nn = idx & (N - 1);
