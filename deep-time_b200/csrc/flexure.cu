@@ -746,6 +746,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   // stores so that a thread keeps FFT_BATCH of them in flight.
   constexpr int NT = RB * N / FFT_EPT;
   static_assert(NT * FFT_EPT == RB * N, "rows: whole pairs per thread");
+  // the raster's width w is 2 N: row offsets use the compile-time 2 N
   if constexpr (RB == 1 && LOGN >= 4) {
     // one row per block: the first stage (radix 16, span 1) straight from global memory, thread
     // j taking pairs n = j + r N/16 (consecutive threads, consecutive pairs)
@@ -755,7 +756,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
     for (int r = 0; r < 16; ++r) {
       z[r] = mk<C>((T)0, (T)0);
       if (row0 < h) {
-        size_t k = (size_t)row0 * w + 2 * (j + r * (N / 16));
+        size_t k = (size_t)row0 * (2 * N) + 2 * (j + r * (N / 16));
         z[r] = *reinterpret_cast<const C*>(v + k);
         if (WEIGHT) {
           C ww = *reinterpret_cast<const C*>(wt + k);
@@ -780,7 +781,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
         int j = row0 + rb;
         C z = mk<C>((T)0, (T)0);
         if (j < h) {
-          size_t k = (size_t)j * w + 2 * nn;
+          size_t k = (size_t)j * (2 * N) + 2 * nn;
           z = *reinterpret_cast<const C*>(v + k);
           if (WEIGHT) {
             C ww = *reinterpret_cast<const C*>(wt + k);
@@ -802,7 +803,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   // split: X[k] = E[k] + W^k O[k], E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
   constexpr int half_n = N / 2 + 1;
 #pragma unroll 2
-  for (int idx = tid; idx < RB * half_n; idx += blockDim.x) {
+  for (int idx = tid; idx < RB * half_n; idx += NT) {
     int rb = idx / half_n, kk = idx - rb * half_n;
     int j = row0 + rb;
     if (j >= h) continue;
@@ -885,7 +886,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   // per column and pair (m, h - m): C[m] = (w_m V[m] + i w_(h-m) V[h-m]) / 2, divide, and back
   constexpr int half_h = h / 2 + 1;
 #pragma unroll 1
-  for (int idx = tid; idx < CPB * half_h; idx += blockDim.x) {
+  for (int idx = tid; idx < CPB * half_h; idx += NT) {
     int cc = idx / half_h, m = idx - cc * half_h;
     int k = k0 + cc;
     if (k >= N) continue;
@@ -946,7 +947,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   if constexpr (LOGH < 4) {
     Stages<C, FFT_EPT, true, LOGH, 1, LOGH, HP, NT>::run(s, tw_inv);
 #pragma unroll 4
-    for (int idx = tid; idx < CPB * h; idx += blockDim.x) {
+    for (int idx = tid; idx < CPB * h; idx += NT) {
       int j = idx >> logc, cc = idx & (CPB - 1);
       int k = k0 + cc;
       if (k >= N) continue;
@@ -1153,7 +1154,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
 #pragma unroll 1
   for (int lv = 0; lv < LEVELS; ++lv) {
   half = half0 + (size_t)lv * h * N;
-  wt = wt0 + (size_t)lv * w * h;
+  wt = wt0 + (size_t)lv * (2 * N) * h;
   if (lv > 0) __syncthreads();  // the previous level's last reads of s are done
 #pragma unroll 1
   for (int base = tid; base < RB * half_n; base += IB * NT) {
@@ -1203,7 +1204,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   // z = x[2 nn] + i x[2 nn + 1] of row j, scaled: the mode's output (the bank's first level
   // stores, the others add to what the same thread stored)
   auto emit = [&](int j, int nn, C z) {
-    size_t k = (size_t)j * w + 2 * nn;
+    size_t k = (size_t)j * (2 * N) + 2 * nn;
     C* o = reinterpret_cast<C*>(out + k);
     if (MODE == INV_STORE) {
       *o = z;
@@ -1249,7 +1250,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   } else {
     smem_fft<C, FFT_EPT, true, LOGN, NT>(s, tw);
 #pragma unroll 4
-    for (int idx = tid; idx < RB * N; idx += blockDim.x) {
+    for (int idx = tid; idx < RB * N; idx += NT) {
       int rb = idx >> logN, nn = idx & (N - 1);
       int j = row0 + rb;
       if (j >= h) continue;
