@@ -845,7 +845,6 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   constexpr int NT = CPB * h / FFT_EPT;
   static_assert(NT * FFT_EPT == CPB * h, "columns: whole values per thread");
   // Makhoul's order: v[p] = x[2p] for p < h/2, x[2(h - 1 - p) + 1] after
-  auto row_of = [](int p) { return p < h / 2 ? 2 * p : 2 * (h - 1 - p) + 1; };
   if constexpr (LOGH < 4) {
     // short columns: gather in Makhoul's order (consecutive threads: consecutive columns)
 #pragma unroll 1
@@ -874,8 +873,11 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
     const int cc = tid & (CPB - 1), j = tid >> logc, k = k0 + cc;
     C v[16];
 #pragma unroll
-    for (int r = 0; r < 16; ++r)
-      v[r] = k < N ? half[(size_t)row_of(j + r * (h / 16)) * N + k] : mk<C>((T)0, (T)0);
+    for (int r = 0; r < 16; ++r) {
+      // j < h / 16, so j + r h / 16 < h / 2 exactly when r < 8: Makhoul's branch is known per r
+      const int p = j + r * (h / 16), row = r < 8 ? 2 * p : 2 * (h - 1 - p) + 1;
+      v[r] = k < N ? half[(size_t)row * N + k] : mk<C>((T)0, (T)0);
+    }
     dft_r<C, 16, false>(v);
     C* col = s + cc * HP;
 #pragma unroll
@@ -979,7 +981,10 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
       dft_r<C, RL, true>(v);
       if (k < N) {
 #pragma unroll
-        for (int r = 0; r < RL; ++r) half[(size_t)row_of(j + r * NSL) * N + k] = cscale(v[r], inv_h);
+        for (int r = 0; r < RL; ++r) {  // j < NSL: the first RL / 2 outputs are even rows
+          const int p = j + r * NSL, row = r < RL / 2 ? 2 * p : 2 * (h - 1 - p) + 1;
+          half[(size_t)row * N + k] = cscale(v[r], inv_h);
+        }
       }
     }
   }
