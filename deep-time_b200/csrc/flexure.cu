@@ -1126,6 +1126,183 @@ __global__ void __launch_bounds__(128) k_row_solve(int N, int h, cplx<T>* __rest
   }
 }
 
+// The row solve in chunks: the down and up recurrences of k_row_solve are linear in their two
+// carried values, so each column is cut into chunks of ROW_CHUNK rows that run in parallel from a
+// zero carry, a short pass per column composes the chunks' 2 x 2 carry transfers (made once per
+// solve, from the factors alone), and a second parallel pass reruns each chunk from its true
+// carry. The same sums as the sequential solve, differently rounded; (chunk, wavenumber)
+// threads, wavenumber fastest, so every row step reads contiguous words.
+constexpr int ROW_CHUNK = 64;
+
+// one row of the down recurrence: x = v - s1 l1 - s2 l2, then (s2, s1) <- (s1, x)
+template <class C, class T>
+__device__ __forceinline__ void row_down(C v, T a1, T a2, C& s1, C& s2) {
+  C x = v;
+  x.x -= s1.x * a1;
+  x.y -= s1.y * a1;
+  x.x -= s2.x * a2;
+  x.y -= s2.y * a2;
+  s2 = s1;
+  s1 = x;
+}
+// the up recurrence's coefficients at row j: l1[j + 1] and l2[j + 2] (0 past the last row)
+template <class T>
+__device__ __forceinline__ void up_coeffs(const T* __restrict__ l1s, const T* __restrict__ l2s, int j, int h, size_t q,
+                                          size_t stride, T& a1, T& a2) {
+  a1 = j + 1 < h ? l1s[(size_t)(j + 1) * stride + q] : (T)0;
+  a2 = j + 2 < h ? l2s[(size_t)(j + 2) * stride + q] : (T)0;
+}
+
+// Per (chunk, wavenumber): the carry transfers of the down recurrence (tf) and of the up one
+// (tb), each the state after the chunk from the unit carries (1, 0) and (0, 1): 4 values apiece,
+// laid out [4][chunks][N + 1].
+template <class T>
+__global__ void __launch_bounds__(128) k_row_transfer(int N, int h, int P, const T* __restrict__ l1s,
+                                                      const T* __restrict__ l2s, T* __restrict__ tf, T* __restrict__ tb) {
+  const size_t stride = (size_t)N + 1, plane = (size_t)P * stride;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= plane) return;
+  const size_t q = t % stride;
+  const int c = (int)(t / stride), a = c * ROW_CHUNK, b = min(h, a + ROW_CHUNK);
+  using C = cplx<T>;
+  // the two unit carries as one complex pair: .x from (1, 0), .y from (0, 1)
+  C s1 = mk<C>((T)1, (T)0), s2 = mk<C>((T)0, (T)1);
+  for (int j = a; j < b; ++j)
+    row_down(mk<C>((T)0, (T)0), l1s[(size_t)j * stride + q], l2s[(size_t)j * stride + q], s1, s2);
+  tf[0 * plane + t] = s1.x;
+  tf[1 * plane + t] = s2.x;
+  tf[2 * plane + t] = s1.y;
+  tf[3 * plane + t] = s2.y;
+  C t1 = mk<C>((T)1, (T)0), t2 = mk<C>((T)0, (T)1);
+  for (int j = b - 1; j >= a; --j) {
+    T a1, a2;
+    up_coeffs(l1s, l2s, j, h, q, stride, a1, a2);
+    row_down(mk<C>((T)0, (T)0), a1, a2, t1, t2);
+  }
+  tb[0 * plane + t] = t1.x;
+  tb[1 * plane + t] = t2.x;
+  tb[2 * plane + t] = t1.y;
+  tb[3 * plane + t] = t2.y;
+}
+
+// The chunk's down recurrence from a zero carry: its end state (s1, s2) into part[2][chunks][N+1]
+template <class T>
+__global__ void __launch_bounds__(128) k_row_down_part(int N, int h, int P, const cplx<T>* __restrict__ half,
+                                                       const T* __restrict__ l1s, const T* __restrict__ l2s,
+                                                       cplx<T>* __restrict__ part, const Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  const size_t stride = (size_t)N + 1, plane = (size_t)P * stride;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= plane) return;
+  const size_t q = t % stride;
+  const int col = q == (size_t)N ? 0 : (int)q;
+  const int c = (int)(t / stride), a = c * ROW_CHUNK, b = min(h, a + ROW_CHUNK);
+  C s1 = mk<C>((T)0, (T)0), s2 = s1;
+#pragma unroll 4
+  for (int j = a; j < b; ++j) row_down(half[(size_t)j * N + col], l1s[(size_t)j * stride + q], l2s[(size_t)j * stride + q], s1, s2);
+  part[t] = s1;
+  part[plane + t] = s2;
+}
+
+// Per wavenumber, the chunks in order (down: first to last; up: last to first): each chunk's
+// true carry-in (carry[2][chunks][N+1]) from the previous one's carry, transfer and zero-carry
+// end state.
+template <class T>
+__global__ void __launch_bounds__(128) k_row_carry(int N, int P, bool up, const T* __restrict__ tr,
+                                                   const cplx<T>* __restrict__ part, cplx<T>* __restrict__ carry,
+                                                   const Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  const size_t stride = (size_t)N + 1, plane = (size_t)P * stride;
+  const size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (q >= stride) return;
+  C s1 = mk<C>((T)0, (T)0), s2 = s1;
+  for (int i = 0; i < P; ++i) {
+    const int c = up ? P - 1 - i : i;
+    const size_t t = (size_t)c * stride + q;
+    carry[t] = s1;
+    carry[plane + t] = s2;
+    const T a1 = tr[0 * plane + t], a2 = tr[1 * plane + t], b1 = tr[2 * plane + t], b2 = tr[3 * plane + t];
+    const C p1 = part[t], p2 = part[plane + t];
+    const C n1 = mk<C>(p1.x + a1 * s1.x + b1 * s2.x, p1.y + a1 * s1.y + b1 * s2.y);
+    const C n2 = mk<C>(p2.x + a2 * s1.x + b2 * s2.x, p2.y + a2 * s1.y + b2 * s2.y);
+    s1 = n1;
+    s2 = n2;
+  }
+}
+
+// The chunk's down recurrence from its true carry, y = x' / dd into the spectrum; then the up
+// recurrence over the chunk from a zero carry, its end state (z[a], z[a+1]) into part
+template <class T>
+__global__ void __launch_bounds__(128) k_row_down_final(int N, int h, int P, cplx<T>* __restrict__ half,
+                                                        const T* __restrict__ dds, const T* __restrict__ l1s,
+                                                        const T* __restrict__ l2s, const cplx<T>* __restrict__ carry,
+                                                        cplx<T>* __restrict__ part, const Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  const size_t stride = (size_t)N + 1, plane = (size_t)P * stride;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= plane) return;
+  const size_t q = t % stride;
+  const int col = q == (size_t)N ? 0 : (int)q;
+  const bool re = q != (size_t)N, im = q != 0;  // column 0's parts belong to two threads
+  const int c = (int)(t / stride), a = c * ROW_CHUNK, b = min(h, a + ROW_CHUNK);
+  C s1 = carry[t], s2 = carry[plane + t];
+#pragma unroll 4
+  for (int j = a; j < b; ++j) {
+    row_down(half[(size_t)j * N + col], l1s[(size_t)j * stride + q], l2s[(size_t)j * stride + q], s1, s2);
+    const T dv = dds[(size_t)j * stride + q];
+    C* o = half + (size_t)j * N + col;
+    if (re && im) {
+      *o = mk<C>(s1.x / dv, s1.y / dv);
+    } else if (re) {
+      o->x = s1.x / dv;
+    } else {
+      o->y = s1.y / dv;
+    }
+  }
+  C t1 = mk<C>((T)0, (T)0), t2 = t1;
+  for (int j = b - 1; j >= a; --j) {
+    T a1, a2;
+    up_coeffs(l1s, l2s, j, h, q, stride, a1, a2);
+    row_down(half[(size_t)j * N + col], a1, a2, t1, t2);
+  }
+  part[t] = t1;
+  part[plane + t] = t2;
+}
+
+// The chunk's up recurrence from its true carry, z into the spectrum
+template <class T>
+__global__ void __launch_bounds__(128) k_row_up_final(int N, int h, int P, cplx<T>* __restrict__ half,
+                                                      const T* __restrict__ l1s, const T* __restrict__ l2s,
+                                                      const cplx<T>* __restrict__ carry, const Scalars* S) {
+  using C = cplx<T>;
+  if (S->stop) return;
+  const size_t stride = (size_t)N + 1, plane = (size_t)P * stride;
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= plane) return;
+  const size_t q = t % stride;
+  const int col = q == (size_t)N ? 0 : (int)q;
+  const bool re = q != (size_t)N, im = q != 0;
+  const int c = (int)(t / stride), a = c * ROW_CHUNK, b = min(h, a + ROW_CHUNK);
+  C t1 = carry[t], t2 = carry[plane + t];
+#pragma unroll 4
+  for (int j = b - 1; j >= a; --j) {
+    T a1, a2;
+    up_coeffs(l1s, l2s, j, h, q, stride, a1, a2);
+    row_down(half[(size_t)j * N + col], a1, a2, t1, t2);
+    C* o = half + (size_t)j * N + col;
+    if (re && im) {
+      *o = t1;
+    } else if (re) {
+      o->x = t1.x;
+    } else {
+      o->y = t1.y;
+    }
+  }
+}
+
 // Inverse rows: Z[k] = E[k] + i O[k] with E = (X[k] + conj X[N-k]) / 2,
 // O = (X[k] - conj X[N-k]) conj(W^k) / 2; x = IFFT_N(Z) / N de-interleaved.
 template <class T, int MODE, int LOGN>
@@ -1399,8 +1576,12 @@ struct Lane {
   // the bank's levels 1 and 2 transform beside level 0, into their own spectra: the three
   // spectra are consecutive (half + k h N), as are the three weights (wt[k] = wt[0] + k n)
   cplx<T>* half_side[2] = {nullptr, nullptr};
-  // the row metric's L D L^T factors per bank level: dd, l1, l2 (h x (N + 1) each)
+  // the row metric's L D L^T factors per bank level: dd, l1, l2 (h x (N + 1) each); when the
+  // rows make more than one chunk, per level the chunks' carry transfers (8 x chunks x (N + 1))
+  // and the chunk states and carries (4 complex x chunks x (N + 1))
   T* row_factors = nullptr;
+  T* row_transfer = nullptr;
+  cplx<T>* row_state = nullptr;
   Tables<T> tab;
   Scalars* S = nullptr;
   cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
@@ -1514,7 +1695,14 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   DT_TRY(dalloc(s, &L.half, 3 * hn));
   L.half_side[0] = L.half + hn;
   L.half_side[1] = L.half + 2 * hn;
-  if (s->metric) DT_TRY(dalloc(s, &L.row_factors, 9 * (size_t)s->h * (s->N + 1)));
+  if (s->metric) {
+    DT_TRY(dalloc(s, &L.row_factors, 9 * (size_t)s->h * (s->N + 1)));
+    const size_t P = ceil_div(s->h, ROW_CHUNK);
+    if (P > 1) {
+      DT_TRY(dalloc(s, &L.row_transfer, 3 * 8 * P * (s->N + 1)));
+      DT_TRY(dalloc(s, &L.row_state, 3 * 4 * P * (s->N + 1)));
+    }
+  }
   DT_TRY(make_tables(s, L.tab));
   DT_TRY(dalloc(s, &L.S, 1));
   DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
@@ -1768,11 +1956,29 @@ static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cp
 template <class T>
 static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, int level, Scalars* S, cudaStream_t st) {
   if (s->metric) {
-    // the row solve per wavenumber with the level's factors (made by setup_precond)
+    // the row solve per wavenumber with the level's factors (made by setup_precond): in chunks
+    // of rows when there is more than one, else one walk per wavenumber
     const size_t fac = (size_t)s->h * (s->N + 1);
     const T* dd = L.row_factors + (size_t)level * 3 * fac;
-    k_row_solve<T><<<ceil_div(s->N + 1, 128), 128, 0, st>>>(s->N, s->h, half, dd, dd + fac, dd + 2 * fac, S);
-    counted();
+    const T *l1 = dd + fac, *l2 = dd + 2 * fac;
+    const int P = (int)ceil_div(s->h, ROW_CHUNK);
+    if (P == 1) {
+      k_row_solve<T><<<ceil_div(s->N + 1, 128), 128, 0, st>>>(s->N, s->h, half, dd, l1, l2, S);
+      counted();
+      return;
+    }
+    const size_t plane = (size_t)P * (s->N + 1);
+    const T* tf = L.row_transfer + (size_t)level * 8 * plane;
+    const T* tb = tf + 4 * plane;
+    cplx<T>* part = L.row_state + (size_t)level * 4 * plane;
+    cplx<T>* carry = part + 2 * plane;
+    const unsigned gp = ceil_div(plane, 128), gq = ceil_div(s->N + 1, 128);
+    k_row_down_part<T><<<gp, 128, 0, st>>>(s->N, s->h, P, half, l1, l2, part, S);
+    k_row_carry<T><<<gq, 128, 0, st>>>(s->N, P, false, tf, part, carry, S);
+    k_row_down_final<T><<<gp, 128, 0, st>>>(s->N, s->h, P, half, dd, l1, l2, carry, part, S);
+    k_row_carry<T><<<gq, 128, 0, st>>>(s->N, P, true, tb, part, carry, S);
+    k_row_up_final<T><<<gp, 128, 0, st>>>(s->N, s->h, P, half, l1, l2, carry, S);
+    for (int k = 0; k < 5; ++k) counted();
     return;
   }
   cols_fn<T>(ilog2(s->h), LogSeq{})<<<g.cgrid, g.cthreads, g.csmem, st>>>(s->N, half, L.tab.tw_col, L.tab.omega, L.tab.lx,
@@ -1976,6 +2182,14 @@ static dt_status setup_precond(dt_flex* s, Lane<T>& L, int precond, int* levels)
       k_row_factor<T><<<ceil_div(s->N + 1, 128), 128, 0, st>>>(s->N, s->h, L.tab.lx, metric_a<T>(s), metric_b<T>(s),
                                                              (T)(1.0 / (s->dx * s->dx)), L.S, k, dd, dd + fac, dd + 2 * fac);
       counted();
+      const int P = (int)ceil_div(s->h, ROW_CHUNK);
+      if (P > 1) {
+        // the chunks' carry transfers, from the factors alone
+        const size_t plane = (size_t)P * (s->N + 1);
+        T* tf = L.row_transfer + (size_t)k * 8 * plane;
+        k_row_transfer<T><<<ceil_div(plane, 128), 128, 0, st>>>(s->N, s->h, P, dd + fac, dd + 2 * fac, tf, tf + 4 * plane);
+        counted();
+      }
     }
   }
   DT_CUDA(cudaGetLastError());

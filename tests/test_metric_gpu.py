@@ -60,9 +60,10 @@ def test_operator_and_bend_on_the_sphere_match_the_oracle(w, h):
 
 
 @pytest.mark.parametrize("precond", [L.PRECOND_REFERENCE, L.PRECOND_MEAN_D])
-@pytest.mark.parametrize("w,h", [(128, 64), (64, 41)])
+@pytest.mark.parametrize("w,h", [(128, 64), (64, 41), (128, 300)])
 def test_the_row_solve_preconditioner_matches_the_oracle(precond, w, h):
-    # h = 41: on the row metric the raster's height need not be a power of two
+    # h = 41: on the row metric the raster's height need not be a power of two; h = 300: the
+    # row solve runs in chunks of 64 rows (the last one of 44)
     dx = 50_000.0
     metric = metric_for(h, dx)
     d, c, r = plate(w, h, 7)
