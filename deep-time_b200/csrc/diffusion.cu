@@ -523,23 +523,158 @@ __global__ void k_lod_rows(int w, int h, int wrap, double* __restrict__ hf, cons
   }
 }
 
-__global__ void k_lod_cols(int w, int h, double* __restrict__ hf, const double* __restrict__ kd, double dtdx2, double* lo,
-                           double* di, double* up, double* cs) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w) return;
-  auto face = [&](int j) -> double {
-    if (j + 1 < h) return 0.5 * (kd[(size_t)j * w + i] + kd[(size_t)(j + 1) * w + i]) * dtdx2;
-    return 0.0;
-  };
-  for (int j = 0; j < h; ++j) {
-    double north = j == 0 ? 0.0 : face(j - 1);
-    double south = face(j);
-    size_t at = (size_t)j * w + i;
-    lo[at] = -north;
-    up[at] = -south;
-    di[at] = 1.0 + north + south;
+// The LOD row pass for wrapping rows with w > 2, on transposed arrays (element (j, i) at i h + j):
+// thread j walks row j, consecutive threads take consecutive rows, so every step reads and writes
+// contiguous words. The arithmetic is k_lod_rows', operation for operation: the coefficients
+// computed on the fly from kd, Sherman-Morrison's two right-hand sides in one elimination
+// (diffusion.rs:1048-1071, :370-419). cT, xT, zT: scratch of w h values; the result into outT.
+__global__ void __launch_bounds__(64) k_lod_rows_wrap_t(int w, int h, double dtdx2, const double* __restrict__ kdT,
+                                                      const double* __restrict__ hfT, double* __restrict__ cT,
+                                                      double* __restrict__ xT, double* __restrict__ zT,
+                                                      double* __restrict__ outT) {
+  constexpr int RB = 8;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= h) return;
+  auto at = [&](int i) { return (size_t)i * h + j; };
+  const double kfirst = kdT[at(0)], klast = kdT[at(w - 1)];
+  const double fw = 0.5 * (klast + kfirst) * dtdx2;  // face(w - 1), across the seam
+  // row 0: west = face(w - 1), east = face(0)
+  double kprev = kfirst;
+  const double east0 = 0.5 * (kfirst + kdT[at(1)]) * dtdx2;
+  const double di0 = 1.0 + fw + east0;
+  const double alpha = -fw, beta = -fw, gamma = -di0;  // up[w-1], lo[0], and -di[0]
+  double bt = di0 - gamma;
+  double xp = hfT[at(0)] / bt, zp = gamma / bt;
+  xT[at(0)] = xp;
+  zT[at(0)] = zp;
+  double west = east0;  // face(i - 1) for the next row
+  kprev = kdT[at(1)];
+  for (int i0 = 1; i0 < w; i0 += RB) {
+    double kn[RB], hv[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int i = min(i0 + u, w - 1);
+      kn[u] = i + 1 < w ? kdT[at(i + 1)] : 0.0;
+      hv[u] = hfT[at(i)];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int i = i0 + u;
+      if (i >= w) break;
+      const double east = i + 1 < w ? 0.5 * (kprev + kn[u]) * dtdx2 : fw;
+      kprev = kn[u];
+      const double lo = -west, upp = -west;  // lo[i] = -face(i - 1) = up[i - 1]
+      double di = 1.0 + west + east;
+      if (i == w - 1) di = di - alpha * beta / gamma;
+      const double c = upp / bt;
+      bt = di - lo * c;
+      xp = (hv[u] - lo * xp) / bt;
+      zp = ((i == w - 1 ? alpha : 0.0) - lo * zp) / bt;
+      cT[at(i)] = c;
+      xT[at(i)] = xp;
+      zT[at(i)] = zp;
+      west = east;
+    }
   }
-  thomas_strided(h, lo, di, up, hf, cs, (size_t)w, (size_t)i);
+  // back substitution, both right-hand sides
+  double xn = xT[at(w - 1)], zn = zT[at(w - 1)];
+  const double xlast = xn, zlast = zn;
+  for (int i0 = w - 2; i0 >= 0; i0 -= RB) {
+    double cn[RB], xv[RB], zv[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int i = max(i0 - u, 0);
+      cn[u] = cT[at(i + 1)];
+      xv[u] = xT[at(i)];
+      zv[u] = zT[at(i)];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int i = i0 - u;
+      if (i < 0) break;
+      xn = xv[u] - cn[u] * xn;
+      zn = zv[u] - cn[u] * zn;
+      xT[at(i)] = xn;
+      zT[at(i)] = zn;
+    }
+  }
+  const double fact = (xn + beta * xlast / gamma) / (1.0 + zn + beta * zlast / gamma);
+#pragma unroll 4
+  for (int i = 0; i < w; ++i) outT[at(i)] = xT[at(i)] - fact * zT[at(i)];
+}
+
+// 32 x 32 tiles through shared memory: out (cols x rows) = the transpose of in (rows x cols)
+__global__ void k_transpose(int rows, int cols, const double* __restrict__ in, double* __restrict__ out) {
+  __shared__ double tile[32][33];
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int r = r0 + k, c = c0 + threadIdx.x;
+    if (r < rows && c < cols) tile[k][threadIdx.x] = in[(size_t)r * cols + c];
+  }
+  __syncthreads();
+  for (int k = threadIdx.y; k < 32; k += blockDim.y) {
+    const int c = c0 + k, r = r0 + threadIdx.x;
+    if (r < rows && c < cols) out[(size_t)c * rows + r] = tile[threadIdx.x][k];
+  }
+}
+
+// The LOD column pass (rows closed, diffusion.rs:420-489): thread i walks column i (consecutive
+// threads, consecutive words), the tridiagonal (1 + north + south, -north, -south) built on the
+// fly and solved by Thomas (diffusion.rs:1029-1046) in place; the Thomas coefficients into cs.
+__global__ void __launch_bounds__(64) k_lod_cols_fast(int w, int h, double* __restrict__ hf, const double* __restrict__ kd,
+                                                    double dtdx2, double* __restrict__ cs) {
+  constexpr int RB = 8;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= w) return;
+  auto at = [&](int j) { return (size_t)j * w + i; };
+  double kcur = kd[at(0)];
+  double south = h > 1 ? 0.5 * (kcur + kd[at(1)]) * dtdx2 : 0.0;
+  double bt = 1.0 + 0.0 + south;  // di[0] = 1 + north + south with north = 0
+  double bp = hf[at(0)] / bt;
+  hf[at(0)] = bp;
+  double north = south;
+  if (h > 1) kcur = kd[at(1)];
+  for (int j0 = 1; j0 < h; j0 += RB) {
+    double kn[RB], hv[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = min(j0 + u, h - 1);
+      kn[u] = j + 1 < h ? kd[at(j + 1)] : 0.0;
+      hv[u] = hf[at(j)];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = j0 + u;
+      if (j >= h) break;
+      const double s2 = j + 1 < h ? 0.5 * (kcur + kn[u]) * dtdx2 : 0.0;
+      kcur = kn[u];
+      const double lo = -north, upp = -north;  // lo[j] = -face(j - 1) = up[j - 1]
+      const double di = 1.0 + north + s2;
+      const double c = upp / bt;
+      bt = di - lo * c;
+      bp = (hv[u] - lo * bp) / bt;
+      cs[at(j)] = c;
+      hf[at(j)] = bp;
+      north = s2;
+    }
+  }
+  double bn = bp;
+  for (int j0 = h - 2; j0 >= 0; j0 -= RB) {
+    double cn[RB], bv[RB];
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = max(j0 - u, 0);
+      cn[u] = cs[at(j + 1)];
+      bv[u] = hf[at(j)];
+    }
+#pragma unroll
+    for (int u = 0; u < RB; ++u) {
+      const int j = j0 - u;
+      if (j < 0) break;
+      bn = bv[u] - cn[u] * bn;
+      hf[at(j)] = bn;
+    }
+  }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -897,10 +1032,21 @@ static dt_status diff_first_guess(dt_diff* s, const dt_diff_params* p, double dt
   DT_CUDA(cudaMemcpyAsync(s->x, s->b, s->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
   if (p->first_guess) {
     double dtdx2 = dt / (s->dx * s->dx);
-    k_lod_rows<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, s->wrap, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
-                                                  s->lod[4], s->lod[5]);
-    k_lod_cols<<<ceil_div(s->w, 64), 64, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[5]);
-    count_launch();
+    if (s->wrap && s->w > 2) {
+      // rows through transposed copies, so each thread's walk reads contiguous words
+      const dim3 tb(32, 8), tg_in(ceil_div(s->w, 32), ceil_div(s->h, 32)), tg_out(ceil_div(s->h, 32), ceil_div(s->w, 32));
+      k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->kd, s->lod[0]);
+      k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->x, s->lod[1]);
+      k_lod_rows_wrap_t<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
+                                                         s->lod[4], s->lod[5]);
+      k_transpose<<<tg_out, tb, 0, st>>>(s->w, s->h, s->lod[5], s->x);
+      for (int k = 0; k < 4; ++k) count_launch();
+    } else {
+      k_lod_rows<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, s->wrap, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2],
+                                                    s->lod[3], s->lod[4], s->lod[5]);
+      count_launch();
+    }
+    k_lod_cols_fast<<<ceil_div(s->w, 64), 64, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[5]);
     count_launch();
   }
   return DT_OK;
@@ -1225,6 +1371,26 @@ dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double
                                                                     s->ap, nullptr, s->partials, s->S64);
   DT_CUDA(cudaGetLastError());
   DT_CUDA(cudaMemcpyAsync(y, s->ap, bytes, cudaMemcpyDeviceToHost, st));
+  DT_CUDA(cudaStreamSynchronize(st));
+  return DT_OK;
+}
+
+// x = the LOD splitting's first guess from h (host arrays; diffusion.rs:370-489)
+dt_status dt_diff_lod(dt_diff* s, const double* h, const double* kd, double dt, double* x) {
+  if (!s || !h || !kd || !x || !(dt > 0.0)) {
+    set_error("dt_diff_lod: bad argument");
+    return DT_BAD_ARG;
+  }
+  size_t bytes = s->n * sizeof(double);
+  cudaStream_t st = s->stream;
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, bytes, cudaMemcpyHostToDevice, st));
+  DT_CUDA(cudaMemcpyAsync(s->b, h, bytes, cudaMemcpyHostToDevice, st));
+  dt_diff_params p;
+  dt_diff_default_params(&p);
+  p.first_guess = 1;
+  DT_TRY(diff_first_guess(s, &p, dt));
+  DT_CUDA(cudaGetLastError());
+  DT_CUDA(cudaMemcpyAsync(x, s->x, bytes, cudaMemcpyDeviceToHost, st));
   DT_CUDA(cudaStreamSynchronize(st));
   return DT_OK;
 }

@@ -51,6 +51,7 @@ def _declare(lib):
         getattr(lib, name).argtypes = [vp, vp, vp, d, ctypes.POINTER(DiffParams), ctypes.POINTER(L.Report)]
     lib.dt_diff_operator.argtypes = [vp, vp, d, vp, vp]
     lib.dt_diff_vcycle.argtypes = [vp, vp, d, i, vp, vp, ctypes.POINTER(i)]
+    lib.dt_diff_lod.argtypes = [vp, vp, vp, d, vp]
     lib._diff_declared = True
 
 
@@ -102,6 +103,13 @@ class Workspace:
         y = np.empty_like(x)
         L.check(L.lib().dt_diff_operator(self._h, _ptr(kd), float(dt), _ptr(x), _ptr(y)))
         return y
+
+    def lod(self, h, kd, dt):
+        """The LOD splitting's first guess from h (diffusion.rs:370-489), as the solve starts from."""
+        h, kd = _f64(h), _f64(kd)
+        x = np.empty_like(h)
+        L.check(L.lib().dt_diff_lod(self._h, _ptr(h), _ptr(kd), float(dt), _ptr(x)))
+        return x
 
     def vcycle(self, kd, dt, r, cycle=L.CYCLE_JACOBI):
         kd, r = _f64(kd), _f64(r)

@@ -164,6 +164,9 @@ dt_status dt_diff_solve_dev(dt_diff* s, double* h_inout, const double* kd, doubl
 dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double* x, double* y);
 /* z = M^-1 r, one V-cycle from z = 0 (FP32 levels), for tests of the cycle; `levels` receives
  * the hierarchy's depth. */
+/* x = the LOD splitting's first guess (diffusion.rs:370-489) from h (host arrays; the solve's own
+ * first guess, for tests) */
+dt_status dt_diff_lod(dt_diff* s, const double* h, const double* kd, double dt, double* x);
 dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, const double* r, float* z, int* levels);
 
 /* ---- learned warm start ----------------------------------------------------------------------

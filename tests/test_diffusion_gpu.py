@@ -136,3 +136,16 @@ def test_the_red_black_cycle_needs_fewer_iterations():
     _, rg = ws.solve_with(topo, kd, 1.0, D.params(cycle=L.CYCLE_RBGS, stop=L.STOP_REL_RESIDUAL, tol=1e-10))
     assert rg.converged and rj.converged
     assert rg.iterations <= rj.iterations, (rg.iterations, rj.iterations)
+
+
+@pytest.mark.parametrize("wrap", [True, False])
+def test_the_lod_first_guess_matches_the_oracle(wrap):
+    # diffusion.rs:370-489: the rows (cyclic when the raster wraps) then the columns, each a
+    # tridiagonal solve; the device takes the same operations in the same order
+    for w, h in [(64, 32), (257, 129), (2048, 64), (3, 5)]:
+        b = terrain(w, h, w + h)
+        kd = shelf_kd(b, 2)
+        ws = D.Workspace(D.Dims(w, h, 2400.0, wrap))
+        got = ws.lod(b, kd, 2.0e6)
+        want = O.diff_lod(b, kd, 2.0e6, 2400.0, wrap)
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), (w, h, wrap)
