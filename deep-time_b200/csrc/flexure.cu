@@ -1524,6 +1524,33 @@ __global__ void k_initial_result(size_t n, T* __restrict__ x, const T* __restric
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += z[k];
 }
 
+// The first preconditioner application when it is already known: the kept first guess's M^-1 r0
+// (or the zero guess's M^-1 b), computed to choose between them, scaled as r was (z = s z). r.z and
+// max|z| go where the application's final pass puts them.
+__global__ void k_scale_given_z(size_t n, float* __restrict__ z, const float* __restrict__ r, const double* scale,
+                                double* partials, Scalars* S) {
+  if (S->stop) return;
+  const float sc = (float)*scale;
+  Acc<2> acc;
+  acc.v[0] = 0.0;
+  acc.v[1] = 0.0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    const float zz = z[k] * sc;
+    z[k] = zz;
+    acc.v[0] += (double)r[k] * (double)zz;
+    acc.v[1] = fmax(acc.v[1], fabs((double)zz));
+  }
+  const int kind[2] = {0, 1};
+  if (reduce_partials<2>(acc, kind, partials, &S->ticket[SITE_PRECOND], gridDim.x) && threadIdx.x == 0)
+    finish_precond(S, acc.v[0], acc.v[1]);
+}
+
+// The zero guess won: its M^-1 b (kept in `zb`) is the first preconditioned residual
+__global__ void k_warm_pick_z(size_t n, float* __restrict__ z, const float* __restrict__ zb, const double* rz) {
+  if (rz[1] < rz[0]) return;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) z[k] = zb[k];
+}
+
 // ---------------------------------------------------------------------------------------------
 // Host side.
 
@@ -2224,10 +2251,19 @@ static dt_status read_scalars(dt_flex* s, const Scalars* S, Scalars* out) {
 // host_loop: 0 the device-side graph loop; 1 a host loop with one sync per iteration; 2 the same
 // with each iteration's scalars printed to stderr. Returns with the solve enqueued (graph) or done.
 template <class T>
-static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop, bool reliable = false) {
+static dt_status run_pcg(dt_flex* s, Lane<T>& L, int levels, int host_loop, bool reliable = false, bool z_given = false) {
   cudaStream_t st = s->stream;
   k_begin<<<1, 1, 0, st>>>(L.S); counted();
-  launch_precondition<T>(s, L, L.r, L.z, levels, st);
+  if constexpr (sizeof(T) == 4) {
+    if (z_given) {
+      // the warm start's choice already preconditioned the first residual (unscaled, in L.z)
+      k_scale_given_z<<<ew_grid(s), 256, 0, st>>>(s->n, L.z, L.r, s->scale, s->partials, L.S); counted();
+    } else {
+      launch_precondition<T>(s, L, L.r, L.z, levels, st);
+    }
+  } else {
+    launch_precondition<T>(s, L, L.r, L.z, levels, st);
+  }
   k_initial_result<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.z, L.S); counted();
   DT_CUDA(cudaMemcpyAsync(L.p, L.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
   if (!host_loop) {
@@ -2332,8 +2368,15 @@ static dt_status warm_or_cold(dt_flex* s, bool warm, Lane<T>& F, int levels) {
     return DT_OK;
   }
   precond_dot<T>(s, F, s->b64, levels, s->rzpair);  // b . M^-1 b
+  if constexpr (sizeof(T) == 4)  // M^-1 b kept (the FP32 lane's ap is free before its loop)
+    DT_CUDA(cudaMemcpyAsync(F.ap, F.z, s->n * sizeof(T), cudaMemcpyDeviceToDevice, st));
   resid64(s);                                       // r0 = b - A x0
   precond_dot<T>(s, F, L.r, levels, s->rzpair + 1);  // r0 . M^-1 r0
+  if constexpr (sizeof(T) == 4) {
+    // F.z: the first preconditioned residual of whichever guess is kept
+    k_warm_pick_z<<<ew_grid(s), 256, 0, st>>>(s->n, F.z, F.ap, s->rzpair);
+    counted();
+  }
   k_warm_decide_pre<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, s->b64, s->rzpair);
   k_warm_record_pre<<<1, 1, 0, st>>>(L.S, s->rzpair, s->warm);
   counted();
@@ -2491,7 +2534,8 @@ static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool 
   k_reliable_init<<<1, 1, 0, st>>>(F.S, L.S, s->scale, p->tol, p->max_iterations, RELIABLE_DELTA,
                                    p->stop == DT_STOP_RMS_RESIDUAL ? 1 : 0);
   counted();
-  DT_TRY(run_pcg<float>(s, F, levels, p->host_loop, true));
+  // warm: the choice's M^-1 r0 (in F.z) is the first preconditioner application
+  DT_TRY(run_pcg<float>(s, F, levels, p->host_loop, true, warm));
   // the correction the FP32 lane holds since its last replacement, and the true residual
   k_accumulate<<<ew_grid(s), 256, 0, st>>>(s->n, L.x, F.x, s->scale); counted();
   resid64(s);
