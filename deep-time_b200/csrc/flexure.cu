@@ -639,22 +639,25 @@ template <class T>
 __global__ void __launch_bounds__(256) k_stats(size_t n, const T* __restrict__ d, const T* __restrict__ c, double dx, int mean_d,
                                                double* partials, Scalars* S) {
   const double RHO_MANTLE = 3300.0;
+  // ln(alpha) rises with d, so its extremes are those of the least and the greatest d: two
+  // evaluations at the end instead of one a cell
   Acc<4> acc;
-  acc.v[0] = -INFINITY;  // -lo as a max
-  acc.v[1] = -INFINITY;  // hi
+  acc.v[0] = -INFINITY;  // -(least d) as a max
+  acc.v[1] = -INFINITY;  // greatest d
   acc.v[2] = 0.0;        // sum c
   acc.v[3] = 0.0;        // sum d
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     double dv = (double)d[k];
-    double la = log(pow(4.0 * fmax(dv, 1e-30) / RHO_MANTLE, 0.25) / dx);
-    acc.v[0] = fmax(acc.v[0], -la);
-    acc.v[1] = fmax(acc.v[1], la);
+    acc.v[0] = fmax(acc.v[0], -dv);
+    acc.v[1] = fmax(acc.v[1], dv);
     acc.v[2] += (double)c[k];
     acc.v[3] += dv;
   }
   const int kind[4] = {1, 1, 0, 0};
-  if (reduce_partials<4>(acc, kind, partials, &S->ticket[SITE_STATS], gridDim.x) && threadIdx.x == 0)
-    finish_stats(S, -acc.v[0], acc.v[1], acc.v[2], acc.v[3], dx, mean_d != 0, n);
+  if (reduce_partials<4>(acc, kind, partials, &S->ticket[SITE_STATS], gridDim.x) && threadIdx.x == 0) {
+    auto la = [&](double dv) { return log(pow(4.0 * fmax(dv, 1e-30) / RHO_MANTLE, 0.25) / dx); };
+    finish_stats(S, la(-acc.v[0]), la(acc.v[1]), acc.v[2], acc.v[3], dx, mean_d != 0, n);
+  }
 }
 
 // Per cell: the bank's weights (squares sum to one) and the damped Jacobi weight 1/2 / diag.
