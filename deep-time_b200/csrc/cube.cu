@@ -195,74 +195,89 @@ __global__ void k_cube_start(size_t cells, const double* __restrict__ h, const d
 }
 
 // ---- the LOD first guess (diffusion.rs:315-381, thomas :1029-1046) ----
-// One thread per face row: the tridiagonal (1 + (ke + kw)/mu, -kw/mu, -ke/mu) by Thomas, the
-// couplings across the face's west and east edges at b's values. cb: the Thomas coefficients.
-__global__ void k_cube_lod_rows(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
-                                const double* __restrict__ mu, const double* __restrict__ b, double* __restrict__ x,
-                                double* __restrict__ cb) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= 6 * n) return;
-  const size_t c0 = (size_t)row * n;
-  auto di = [&](size_t c) { return __dadd_rn(1.0, __ddiv_rn(__dadd_rn(k[c * 8 + 0], k[c * 8 + 4]), mu[c])); };
-  auto rhs = [&](int i) {
-    const size_t c = c0 + i;
+// Face rows, then face columns, each a tridiagonal (1 + (k_a + k_b)/mu, -k_a/mu, -k_b/mu) solved
+// by Thomas, the couplings across a face's edge taken at the old values (b for the rows, the
+// rows' answer for the columns).
+// Every walk reads contiguous words: k_cube_lod_prep lays out, per cell, the row systems'
+// coefficients and right-hand side in face-transposed order (cell (f, i, j) at f n^2 + i n + j,
+// so that consecutive face rows are consecutive words) and the column systems' coefficients in
+// the cells' own order.
+__global__ void k_cube_lod_prep(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                const double* __restrict__ mu, const double* __restrict__ b, double* __restrict__ rloT,
+                                double* __restrict__ rupT, double* __restrict__ rdiT, double* __restrict__ rbT,
+                                double* __restrict__ clo, double* __restrict__ cup, double* __restrict__ cdi) {
+  const size_t nn = (size_t)n * n, cells = 6 * nn;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    const size_t f = c / nn, rest = c % nn, j = rest / n, i = rest % n, t = f * nn + i * n + j;
+    const double ke = k[c * 8 + 0], kw = k[c * 8 + 4], kn = k[c * 8 + 2], ks = k[c * 8 + 6], m = mu[c];
+    rloT[t] = __ddiv_rn(-kw, m);
+    rupT[t] = __ddiv_rn(-ke, m);
+    rdiT[t] = __dadd_rn(1.0, __ddiv_rn(__dadd_rn(ke, kw), m));
     double v = b[c];
-    if (i == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 4], b[slots[c * 8 + 4]]), mu[c]));
-    if (i == n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 0], b[slots[c * 8 + 0]]), mu[c]));
-    return v;
-  };
-  double beta = di(c0);
-  double prev = __ddiv_rn(rhs(0), beta);
-  x[c0] = prev;
-  for (int i = 1; i < n; ++i) {
-    const size_t c = c0 + i;
-    const double up = __ddiv_rn(-k[(c - 1) * 8 + 0], mu[c - 1]);
-    const double lo = __ddiv_rn(-k[c * 8 + 4], mu[c]);
-    const double ci = __ddiv_rn(up, beta);
-    cb[c] = ci;
-    beta = __dsub_rn(di(c), __dmul_rn(lo, ci));
-    prev = __ddiv_rn(__dsub_rn(rhs(i), __dmul_rn(lo, prev)), beta);
-    x[c] = prev;
-  }
-  for (int i = n - 2; i >= 0; --i) {
-    const size_t c = c0 + i;
-    x[c] = __dsub_rn(x[c], __dmul_rn(cb[c + 1], x[c + 1]));
+    if (i == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(kw, b[slots[c * 8 + 4]]), m));
+    if (i == (size_t)n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(ke, b[slots[c * 8 + 0]]), m));
+    rbT[t] = v;
+    clo[c] = __ddiv_rn(-kn, m);
+    cup[c] = __ddiv_rn(-ks, m);
+    cdi[c] = __dadd_rn(1.0, __ddiv_rn(__dadd_rn(kn, ks), m));
   }
 }
 
-// One thread per face column: the same along j (N = slot 2, S = slot 6) from the rows' result
-// y, into out (column-major per face: column f n + i at out + (f n + i) n).
-__global__ void k_cube_lod_cols(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
-                                const double* __restrict__ mu, const double* __restrict__ y, double* __restrict__ out,
-                                double* __restrict__ cb) {
+// Thomas along a line of n values at base + r * stride (r = 0 .. n - 1): x from the line's
+// lo, up, di and right-hand side; c: the coefficients (diffusion.rs:1029-1046)
+__device__ __forceinline__ void thomas_line(int n, size_t base, size_t stride, const double* __restrict__ lo,
+                                            const double* __restrict__ up, const double* __restrict__ di,
+                                            const double* __restrict__ rhs, double* __restrict__ x,
+                                            double* __restrict__ c) {
+  double beta = di[base];
+  double prev = __ddiv_rn(rhs[base], beta);
+  x[base] = prev;
+  for (int r = 1; r < n; ++r) {
+    const size_t at = base + (size_t)r * stride;
+    const double ci = __ddiv_rn(up[at - stride], beta);
+    c[at] = ci;
+    beta = __dsub_rn(di[at], __dmul_rn(lo[at], ci));
+    prev = __ddiv_rn(__dsub_rn(rhs[at], __dmul_rn(lo[at], prev)), beta);
+    x[at] = prev;
+  }
+  double next = prev;
+  for (int r = n - 2; r >= 0; --r) {
+    const size_t at = base + (size_t)r * stride;
+    next = __dsub_rn(x[at], __dmul_rn(c[at + stride], next));
+    x[at] = next;
+  }
+}
+
+// Face rows in transposed order: thread (f, j) walks i at f n^2 + i n + j
+__global__ void k_cube_lod_rows_t(int n, const double* __restrict__ loT, const double* __restrict__ upT,
+                                  const double* __restrict__ diT, const double* __restrict__ bT, double* __restrict__ xT,
+                                  double* __restrict__ cT) {
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= 6 * n) return;
+  const size_t nn = (size_t)n * n, f = row / n, j = row % n;
+  thomas_line(n, f * nn + j, (size_t)n, loT, upT, diT, bT, xT, cT);
+}
+
+// Face columns in the cells' order: thread (f, i) walks j at f n^2 + j n + i; the right-hand
+// side y plus the couplings across the face's north and south edges at y's values (into rhs)
+__global__ void k_cube_lod_cols_rhs(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
+                                    const double* __restrict__ mu, const double* __restrict__ y, double* __restrict__ rhs) {
+  const size_t nn = (size_t)n * n, cells = 6 * nn;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < cells; c += (size_t)gridDim.x * blockDim.x) {
+    const size_t j = (c % nn) / n;
+    double v = y[c];
+    if (j == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 2], y[slots[c * 8 + 2]]), mu[c]));
+    if (j == (size_t)n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 6], y[slots[c * 8 + 6]]), mu[c]));
+    rhs[c] = v;
+  }
+}
+__global__ void k_cube_lod_cols_f(int n, const double* __restrict__ lo, const double* __restrict__ up,
+                                  const double* __restrict__ di, const double* __restrict__ rhs, double* __restrict__ x,
+                                  double* __restrict__ c) {
   const int col = blockIdx.x * blockDim.x + threadIdx.x;
   if (col >= 6 * n) return;
   const size_t nn = (size_t)n * n, f = col / n, i = col % n;
-  auto cell = [&](int j) { return f * nn + (size_t)j * n + i; };
-  auto di = [&](size_t c) { return __dadd_rn(1.0, __ddiv_rn(__dadd_rn(k[c * 8 + 2], k[c * 8 + 6]), mu[c])); };
-  auto rhs = [&](int j) {
-    const size_t c = cell(j);
-    double v = y[c];
-    if (j == 0) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 2], y[slots[c * 8 + 2]]), mu[c]));
-    if (j == n - 1) v = __dadd_rn(v, __ddiv_rn(__dmul_rn(k[c * 8 + 6], y[slots[c * 8 + 6]]), mu[c]));
-    return v;
-  };
-  double* o = out + (size_t)col * n;
-  double* cc = cb + (size_t)col * n;
-  double beta = di(cell(0));
-  double prev = __ddiv_rn(rhs(0), beta);
-  o[0] = prev;
-  for (int j = 1; j < n; ++j) {
-    const size_t c = cell(j), cp = cell(j - 1);
-    const double up = __ddiv_rn(-k[cp * 8 + 6], mu[cp]);
-    const double lo = __ddiv_rn(-k[c * 8 + 2], mu[c]);
-    const double ci = __ddiv_rn(up, beta);
-    cc[j] = ci;
-    beta = __dsub_rn(di(c), __dmul_rn(lo, ci));
-    prev = __ddiv_rn(__dsub_rn(rhs(j), __dmul_rn(lo, prev)), beta);
-    o[j] = prev;
-  }
-  for (int j = n - 2; j >= 0; --j) o[j] = __dsub_rn(o[j], __dmul_rn(cc[j + 1], o[j + 1]));
+  thomas_line(n, f * nn + i, (size_t)n, lo, up, di, rhs, x, c);
 }
 
 // x (face row-major) from the column pass's face-column-major result
@@ -485,6 +500,7 @@ struct dt_cube {
   double *kd = nullptr, *h = nullptr;  // staging for the host entry points
   double *k = nullptr, *s = nullptr, *diag = nullptr;
   double *rhs = nullptr, *x = nullptr, *b = nullptr, *tmp = nullptr, *cb = nullptr;
+  double* lodw[7] = {};  // the LOD's row systems (transposed) and column systems
   double *r = nullptr, *z = nullptr, *po = nullptr, *pn = nullptr, *ap = nullptr;
   double* partials = nullptr;
   double* sc = nullptr;  // scalars: 0 rr, 1 pap, 2 rz, 3 rz_new, 4 alpha, 5 beta, 6 lost, 7 weight, 8 kk, 9 rhs.rhs,
@@ -605,9 +621,14 @@ dt_status cube_precondition(dt_cube* s) {
 // the LOD first guess: x from b (diffusion.rs:315-381)
 void cube_lod(dt_cube* s, const double* b, double* x) {
   const int rows = 6 * s->n;
-  k_cube_lod_rows<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, b, x, s->cb);
-  k_cube_lod_cols<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, x, s->tmp, s->cb);
+  double** w = s->lodw;
+  // the systems laid out for contiguous walks; the rows' answer comes back transposed in tmp
+  k_cube_lod_prep<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, b, w[0], w[1], w[2], w[3], w[4],
+                                                              w[5], w[6]);
+  k_cube_lod_rows_t<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, w[0], w[1], w[2], w[3], s->tmp, s->cb);
   k_cube_untranspose<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->tmp, x);
+  k_cube_lod_cols_rhs<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, x, w[3]);
+  k_cube_lod_cols_f<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, w[4], w[5], w[6], w[3], x, s->cb);
 }
 
 // One device scalar to the host (a sync); a device error reads as NaN, which ends the loop and
@@ -793,6 +814,8 @@ dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const 
   if ((st = cube_alloc(s, &s->k, cells * 8)) != DT_OK) return fail(st);
   for (double** p : {&s->kd, &s->h, &s->s, &s->diag, &s->rhs, &s->x, &s->b, &s->tmp, &s->cb, &s->r, &s->z, &s->po, &s->pn, &s->ap})
     if ((st = cube_alloc(s, p, cells)) != DT_OK) return fail(st);
+  for (double*& p : s->lodw)
+    if ((st = cube_alloc(s, &p, cells)) != DT_OK) return fail(st);
   if ((st = cube_alloc(s, &s->partials, 2 * CUBE_RED_BLOCKS)) != DT_OK) return fail(st);
   if ((st = cube_alloc(s, &s->sc, 16)) != DT_OK) return fail(st);
   // the hierarchy (multigrid.rs:170-186): coarsen while a level has more than 64 cells and a side
