@@ -528,11 +528,11 @@ __global__ void k_lod_rows(int w, int h, int wrap, double* __restrict__ hf, cons
 // contiguous words. The arithmetic is k_lod_rows', operation for operation: the coefficients
 // computed on the fly from kd, Sherman-Morrison's two right-hand sides in one elimination
 // (diffusion.rs:1048-1071, :370-419). cT, xT, zT: scratch of w h values; the result into outT.
-__global__ void __launch_bounds__(64) k_lod_rows_wrap_t(int w, int h, double dtdx2, const double* __restrict__ kdT,
+__global__ void __launch_bounds__(32) k_lod_rows_wrap_t(int w, int h, double dtdx2, const double* __restrict__ kdT,
                                                       const double* __restrict__ hfT, double* __restrict__ cT,
                                                       double* __restrict__ xT, double* __restrict__ zT,
-                                                      double* __restrict__ outT) {
-  constexpr int RB = 8;
+                                                      double* __restrict__ fact_out) {
+  constexpr int RB = 16;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= h) return;
   auto at = [&](int i) { return (size_t)i * h + j; };
@@ -598,9 +598,16 @@ __global__ void __launch_bounds__(64) k_lod_rows_wrap_t(int w, int h, double dtd
       zT[at(i)] = zn;
     }
   }
-  const double fact = (xn + beta * xlast / gamma) / (1.0 + zn + beta * zlast / gamma);
-#pragma unroll 4
-  for (int i = 0; i < w; ++i) outT[at(i)] = xT[at(i)] - fact * zT[at(i)];
+  // Sherman-Morrison's factor; k_lod_rows_combine forms x - fact z with every thread of the GPU
+  fact_out[j] = (xn + beta * xlast / gamma) / (1.0 + zn + beta * zlast / gamma);
+}
+
+// out = x - fact z per cell of the transposed rows (element (j, i) at i h + j)
+__global__ void k_lod_rows_combine(int w, int h, const double* __restrict__ xT, const double* __restrict__ zT,
+                                   const double* __restrict__ fact, double* __restrict__ outT) {
+  const size_t n = (size_t)w * h;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+    outT[k] = xT[k] - fact[k % h] * zT[k];
 }
 
 // 32 x 32 tiles through shared memory: out (cols x rows) = the transpose of in (rows x cols)
@@ -621,9 +628,9 @@ __global__ void k_transpose(int rows, int cols, const double* __restrict__ in, d
 // The LOD column pass (rows closed, diffusion.rs:420-489): thread i walks column i (consecutive
 // threads, consecutive words), the tridiagonal (1 + north + south, -north, -south) built on the
 // fly and solved by Thomas (diffusion.rs:1029-1046) in place; the Thomas coefficients into cs.
-__global__ void __launch_bounds__(64) k_lod_cols_fast(int w, int h, double* __restrict__ hf, const double* __restrict__ kd,
+__global__ void __launch_bounds__(32) k_lod_cols_fast(int w, int h, double* __restrict__ hf, const double* __restrict__ kd,
                                                     double dtdx2, double* __restrict__ cs) {
-  constexpr int RB = 8;
+  constexpr int RB = 16;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= w) return;
   auto at = [&](int j) { return (size_t)j * w + i; };
@@ -1037,16 +1044,18 @@ static dt_status diff_first_guess(dt_diff* s, const dt_diff_params* p, double dt
       const dim3 tb(32, 8), tg_in(ceil_div(s->w, 32), ceil_div(s->h, 32)), tg_out(ceil_div(s->h, 32), ceil_div(s->w, 32));
       k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->kd, s->lod[0]);
       k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->x, s->lod[1]);
-      k_lod_rows_wrap_t<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
+      // the walks leave x, z and each row's Sherman-Morrison factor (lod[5]); one parallel pass combines them
+      k_lod_rows_wrap_t<<<ceil_div(s->h, 32), 32, 0, st>>>(s->w, s->h, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
                                                          s->lod[4], s->lod[5]);
-      k_transpose<<<tg_out, tb, 0, st>>>(s->w, s->h, s->lod[5], s->x);
-      for (int k = 0; k < 4; ++k) count_launch();
+      k_lod_rows_combine<<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, s->lod[3], s->lod[4], s->lod[5], s->lod[1]);
+      k_transpose<<<tg_out, tb, 0, st>>>(s->w, s->h, s->lod[1], s->x);
+      for (int k = 0; k < 5; ++k) count_launch();
     } else {
       k_lod_rows<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, s->wrap, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2],
                                                     s->lod[3], s->lod[4], s->lod[5]);
       count_launch();
     }
-    k_lod_cols_fast<<<ceil_div(s->w, 64), 64, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[5]);
+    k_lod_cols_fast<<<ceil_div(s->w, 32), 32, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[5]);
     count_launch();
   }
   return DT_OK;
