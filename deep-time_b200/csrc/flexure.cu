@@ -1648,9 +1648,11 @@ struct dt_flex {
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
   // and box shape, made on first use
   bool tma = false;
-  // the sphere's row metric (RowMetric): a (h values) and b (h + 1) in both precisions; null for
-  // the block metric
-  bool metric = false;
+  // the sphere's row metric (RowMetric): a (h values) and b (h + 1) in both precisions; for the
+  // block metric with a height that is not a power of two, the block metric's own couplings
+  // (a = 1, b = 1 inside, 0 at the raster's edges), for the row solve only
+  bool metric = false;     // the operator and the Jacobi weights on the row metric
+  bool row_solve = false;  // the spectral pass along y by the per-wavenumber row solve
   double *met_a64 = nullptr, *met_b64 = nullptr;
   float *met_a32 = nullptr, *met_b32 = nullptr;
   // the bank levels' side streams and their fork / join events
@@ -1725,7 +1727,7 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   DT_TRY(dalloc(s, &L.half, 3 * hn));
   L.half_side[0] = L.half + hn;
   L.half_side[1] = L.half + 2 * hn;
-  if (s->metric) {
+  if (s->row_solve) {
     DT_TRY(dalloc(s, &L.row_factors, 9 * (size_t)s->h * (s->N + 1)));
     const size_t P = ceil_div(s->h, ROW_CHUNK);
     if (P > 1) {
@@ -1985,7 +1987,7 @@ static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cp
 }
 template <class T>
 static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, int level, Scalars* S, cudaStream_t st) {
-  if (s->metric) {
+  if (s->row_solve) {
     // the row solve per wavenumber with the level's factors (made by setup_precond): in chunks
     // of rows when there is more than one, else one walk per wavenumber
     const size_t fac = (size_t)s->h * (s->N + 1);
@@ -2201,10 +2203,10 @@ static dt_status setup_precond(dt_flex* s, Lane<T>& L, int precond, int* levels)
   DT_CUDA(cudaStreamSynchronize(st));
   if (lv == 3) {
     k_bank_weights<T><<<ew_grid(s), 256, 0, st>>>(s->w, s->h, L.d, L.c, s->dx, L.wt[0], L.wt[1], L.wt[2], L.J, L.S,
-                                                   s->met_a64, s->met_b64);
+                                                   s->metric ? s->met_a64 : nullptr, s->metric ? s->met_b64 : nullptr);
     counted();
   }
-  if (s->metric) {
+  if (s->row_solve) {
     // the row solve's factors of each level (its d, the bank's c_ref)
     const size_t fac = (size_t)s->h * (s->N + 1);
     for (int k = 0; k < lv; ++k) {
@@ -2631,11 +2633,12 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     set_error("dt_flex_create: bad raster %d x %d, dx %g", w, h, dx);
     return DT_BAD_ARG;
   }
-  // the cosine transform along y needs h a power of two; on the row metric y is solved per
-  // wavenumber instead, so any h will do
-  if ((w & 1) || !is_pow2(w / 2) || w / 2 > 8192 || h > 8192 || (!metric_a && !is_pow2(h))) {
-    set_error("dt_flex_create: the device transforms need w/2 (and, for the block metric, h) powers of two, at most "
-              "8192 (got %d x %d)", w, h);
+  // the transform along x needs w/2 a power of two; along y the cosine transform needs h one,
+  // and any other h is solved per wavenumber (the row solve, with the block metric's couplings
+  // when no metric is given)
+  if ((w & 1) || !is_pow2(w / 2) || w / 2 > 8192 || h > 8192) {
+    set_error("dt_flex_create: the device transforms need w/2 a power of two, at most 8192, and h at most 8192 "
+              "(got %d x %d)", w, h);
     return DT_UNSUPPORTED;
   }
   if (!metric_a != !metric_b) {
@@ -2677,9 +2680,22 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     return fail(DT_DEVICE_ERROR);
   }
   s->own_stream = true;
-  if (metric_a) {
-    // the sphere's row metric (RowMetric, flexure.rs:954-998), in both lanes' precisions
+  // RowMetric::block (flexure.rs:1000-1010): the block metric's couplings, for a height the
+  // cosine transform does not take
+  std::vector<double> block_a, block_b;
+  if (!metric_a && !is_pow2(h)) {
+    block_a.assign(h, 1.0);
+    block_b.assign(h + 1, 1.0);
+    block_b[0] = block_b[h] = 0.0;
+    metric_a = block_a.data();
+    metric_b = block_b.data();
+  } else if (metric_a) {
     s->metric = true;
+  }
+  if (metric_a) {
+    // the sphere's row metric (RowMetric, flexure.rs:954-998), or the block one, in both lanes'
+    // precisions
+    s->row_solve = true;
     std::vector<float> a32(metric_a, metric_a + h), b32(metric_b, metric_b + h + 1);
     if ((st = dalloc(s, &s->met_a64, (size_t)h)) != DT_OK || (st = dalloc(s, &s->met_b64, (size_t)h + 1)) != DT_OK ||
         (st = dalloc(s, &s->met_a32, (size_t)h)) != DT_OK || (st = dalloc(s, &s->met_b32, (size_t)h + 1)) != DT_OK)

@@ -254,3 +254,36 @@ def test_the_longest_transforms_match_the_oracle(w, h, precision):
         want = O.flex_precondition(d, c, r, dx, precond)
         bound = (1e-12 if precond == L.PRECOND_MEAN_D else 1e-8) if precision == L.PREC_FP64 else 5e-5
         assert rel_l2(z, want) < bound, (precond, rel_l2(z, want))
+
+
+@pytest.mark.parametrize("w,h", [(64, 41), (128, 82), (256, 300)])
+def test_heights_that_are_not_powers_of_two_match_the_oracle(w, h):
+    # The block metric at a height the cosine transform does not take: along y each wavenumber
+    # is solved by the row solve with the block metric's couplings (RowMetric::block,
+    # flexure.rs:1000-1010), which is that transform's inverse; the Jacobi weights stay the block
+    # metric's. The oracle takes its own Bluestein route for such heights.
+    dx = 20_000.0
+    d = rigidity(patchy(w, h, 5.0, 60.0))
+    c = np.where(np.arange(w)[None, :] < w // 3, RHO_M - 1030.0, RHO_M) * np.ones((h, 1))
+    r = np.random.default_rng(h).standard_normal((h, w)) * 1e4
+    sv = F.Solver(w, h, dx)
+    for precond in (L.PRECOND_MEAN_D, L.PRECOND_REFERENCE):
+        want = O.flex_precondition(d, c, r, dx, precond)
+        z = sv.precondition(d, c, r, precond, L.PREC_FP64)
+        assert rel_l2(z, want) < (1e-10 if precond == L.PRECOND_MEAN_D else 1e-8), precond
+        z32 = sv.precondition(d, c, r, precond, L.PREC_MIXED)
+        assert rel_l2(z32, want) < 5e-5, precond
+
+
+def test_the_production_raster_takes_the_reference_rule_like_the_oracle():
+    # the timestep's flexure raster (1024 x 328 at the reference's 39 km cells): the max|z| rule
+    # at 2 m, 60 iterations, the reference preconditioner
+    w, h, dx = 1024, 328, 39_000.0
+    d, c, _ = I.flexure_problem(w, h, 8.0, 328)
+    b = np.zeros((h, w))
+    b.ravel()[::97] = RHO_M * 2500.0
+    x, rep = F.Solver(w, h, dx).solve(d, c, b, 2.0, 60)
+    xo, ro = O.flex_solve(d, c, b, dx, 2.0, 60)
+    assert rep.converged and ro["converged"], (rep, ro)
+    assert abs(rep.iterations - ro["iterations"]) <= 1, (rep, ro)
+    assert rel_l2(x, xo) < 1e-6
