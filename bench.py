@@ -18,6 +18,9 @@ throughput over the max-over-ranks device time.
   roofline  the dominant kernel's algorithmic bytes per launch / its event-timed launch duration
   cpu_baseline  the oracle (a C++ restatement of the reference's CPU solver, FP64, its own
             3-level bank preconditioner) on the host's cores, a bounded sample extrapolated
+  step_raster  the timestep's own call at 1024 x 328 (39 km cells, max|z| < 2 m, at most 60
+            iterations), FP64, device and end to end; the oracle's time for the same
+            call sits in cpu_baseline
 --impl reference times that CPU restatement alone, as the reference arm.
 """
 from __future__ import annotations
@@ -61,6 +64,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error against the oracle's 1e-12 solve")
     ap.add_argument("--no-diffusion", action="store_true", help="skip the diffusion solve's leg")
+    ap.add_argument("--no-step-raster", action="store_true",
+                    help="skip the timestep raster's leg (1024 x 328, the reference's max|z| rule)")
     ap.add_argument("--warm", default="unet" if os.path.exists(WEIGHTS) else "none", choices=["unet", "none"],
                     help="first guess of the benchmarked solve (default: the U-Net when trained weights exist)")
     ap.add_argument("--weights", default=WEIGHTS)
@@ -197,6 +202,71 @@ def oracle_cpu_baseline(d, c, b, its_needed, max_seconds=30.0):
                        f"iterations, extrapolated to {its_needed} iterations (the count the same algorithm takes to "
                        f"1e-8 on the GPU); OpenMP on all {os.cpu_count()} host threads"),
             "seconds_per_solve": seconds}
+
+
+STEP_W, STEP_H, STEP_DX = 1024, 328, 39_000.0
+STEP_TOL_M, STEP_MAX_IT = 2.0, 60
+
+
+def step_inputs(k=2):
+    from deeptime_gpu import inputs as I
+
+    return [I.flexure_problem(STEP_W, STEP_H, 8.0, 5000 + 100 * i) for i in range(k)]
+
+
+def oracle_step_seconds(sets):
+    """The oracle's time per solve of the timestep raster's call (the reference preconditioner,
+    max|z| < 2 m, at most 60 iterations), setup included, over the given input sets."""
+    from oracle import oracle as O
+
+    t = time.perf_counter()
+    its = [O.flex_solve(d, c, b, STEP_DX, STEP_TOL_M, STEP_MAX_IT)[1]["iterations"] for d, c, b in sets]
+    return (time.perf_counter() - t) / len(sets), its
+
+
+def step_raster_leg(lib, stream, timed, max_over_ranks, world, steps, sets):
+    """The timestep's own flexure call on its own raster: 1024 x 328 cells of 39 km (a height
+    the cosine transform does not take, so y goes through the row solve with the block
+    couplings), the reference preconditioner, max|z| < 2 m, at most 60 iterations, from x = 0.
+    FP64, the reference's arithmetic (the mixed paths stop on residual rules only); device time
+    per solve with inputs resident, and end to end through dt_flex_solve from pinned host
+    buffers."""
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import flexure as F
+
+    sv = F.Solver(STEP_W, STEP_H, STEP_DX)
+    L.check(lib.dt_flex_set_stream(sv._h, ctypes.c_void_p(stream.cuda_stream)))
+    dev = [tuple(torch.from_numpy(a).cuda() for a in s) for s in sets]
+    host = [tuple(torch.from_numpy(a).pin_memory() for a in s) for s in sets]
+    x_dev = torch.zeros((STEP_H, STEP_W), dtype=torch.float64, device="cuda")
+    x_host = torch.zeros((STEP_H, STEP_W), dtype=torch.float64).pin_memory()
+
+    def call(fn, arrays, x, p):
+        d, c, b = arrays
+        rep = L.Report()
+        L.check(fn(sv._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(c.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                   ctypes.c_void_p(x.data_ptr()), ctypes.byref(p), ctypes.byref(rep)))
+        return rep
+
+    out = {"workload": f"flexure::step's solve, {STEP_W}x{STEP_H} at {STEP_DX / 1e3:g} km, reference 3-level bank + "
+                       f"Jacobi, max|z| < {STEP_TOL_M:g} m, at most {STEP_MAX_IT} iterations, x = 0",
+           "inputs": f"{len(sets)} seeded input sets cycled (rigidity sigma 8 cells, |k|^-2 topography of std 1500 m)"}
+    for name, prec in (("fp64", L.PREC_FP64),):
+        p = F.params(precision=prec, tol=STEP_TOL_M, max_iterations=STEP_MAX_IT)
+        call(lib.dt_flex_solve_dev, dev[0], x_dev, p)
+        ms, reps = timed(lambda i: call(lib.dt_flex_solve_dev, dev[i % len(dev)], x_dev, p), steps)
+        ms = max_over_ranks(ms, world) / steps
+        call(lib.dt_flex_solve, host[0], x_host, p)
+        ems, _ = timed(lambda i: call(lib.dt_flex_solve, host[i % len(host)], x_host, p), steps)
+        ems = max_over_ranks(ems, world) / steps
+        out[name] = {"ms_per_solve": ms, "e2e_ms_per_solve": ems,
+                     "iterations": statistics.mean(r.iterations for r in reps),
+                     "converged": all(r.converged for r in reps),
+                     "max_error_m": max(r.error_m for r in reps)}
+    sv.close()
+    return out
 
 
 def run_reference(args, rank, world):
@@ -394,12 +464,22 @@ def main():
     }
     if not args.no_diffusion:
         line["diffusion"] = diffusion_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4))
+    step_sets = None
+    if not args.no_step_raster:
+        step_sets = step_inputs()
+        line["step_raster"] = step_raster_leg(lib, stream, timed, max_over_ranks, world, args.steps, step_sets)
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy(lambda p: (solve_dev(0, p), x_dev.cpu().numpy())[1], head, methods, inputs[0])
     if rank == 0 and not args.no_cpu_baseline:
         d, c, b = inputs[0]
         ref_its = breakdown["fp64_bank_gpu"]["iterations"]
         line["cpu_baseline"] = oracle_cpu_baseline(d, c, b, int(round(ref_its)))
+        if step_sets is not None:
+            secs, its = oracle_step_seconds(step_sets)
+            line["cpu_baseline"]["step_raster"] = {
+                "ms_per_solve": secs * 1e3, "iterations": its,
+                "sample": f"the oracle's solve of the step raster's call on each of its {len(step_sets)} input sets, "
+                          f"setup included, OpenMP on all {os.cpu_count()} host threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     sv.close()

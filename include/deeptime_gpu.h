@@ -102,7 +102,10 @@ void dt_flex_default_params(dt_flex_params* p);
  * one without the other is DT_BAD_ARG. On the row metric the operator runs the per-block stencil
  * with the rows' couplings, the Jacobi weights take (L D L)'s diagonal on the metric, and the
  * spectral pass solves d L_k^2 + c per wavenumber along y (RowSolve, :1012-1099) in place of the
- * cosine transform, so h need not be a power of two (w/2 still must). */
+ * cosine transform, so h need not be a power of two (w/2 still must). On the block metric a
+ * height that is not a power of two takes the same row solve with the block couplings
+ * (RowMetric::block: a = 1, b = 1 inside and 0 at the edges), the cosine transform's inverse;
+ * the operator and the Jacobi weights stay the block metric's. */
 dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const double* metric_b, dt_flex** out);
 dt_status dt_flex_destroy(dt_flex* s);
 /* Binds the handle to a CUDA stream (cudaStream_t passed as void*); NULL = the handle's own. */
