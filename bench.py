@@ -21,6 +21,10 @@ throughput over the max-over-ranks device time.
   step_raster  the timestep's own call at 1024 x 328 (39 km cells, max|z| < 2 m, at most 60
             iterations), FP64, device and end to end; the oracle's time for the same
             call sits in cpu_baseline
+  grid_helpers  the step's restrict / prolong / binomial / box blur on an 8192 x 4096 raster,
+            each call's bandwidth over its algorithmic bytes
+  cube      the cube grid's diffusion at 6 x 256^2 cells, device and end to end; the oracle's
+            time beside it in cpu_baseline
 --impl reference times that CPU restatement alone, as the reference arm.
 """
 from __future__ import annotations
@@ -64,6 +68,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error against the oracle's 1e-12 solve")
     ap.add_argument("--no-diffusion", action="store_true", help="skip the diffusion solve's leg")
+    ap.add_argument("--no-helpers", action="store_true",
+                    help="skip the legs of the step's grid helpers and the cube grid's diffusion")
     ap.add_argument("--no-step-raster", action="store_true",
                     help="skip the timestep raster's leg (1024 x 328, the reference's max|z| rule)")
     ap.add_argument("--warm", default="unet" if os.path.exists(WEIGHTS) else "none", choices=["unet", "none"],
@@ -269,6 +275,118 @@ def step_raster_leg(lib, stream, timed, max_over_ranks, world, steps, sets):
     return out
 
 
+GRID_W, GRID_H = 8192, 4096
+CUBE_N, CUBE_TOL_M, CUBE_DTS = 256, 1e-6, (7.0, 60.0)
+
+
+def grid_leg(lib, stream, timed, max_over_ranks, world, steps, peak):
+    """The step's grid helpers on a device raster of 8192 x 4096 FP64 cells (268 MB, larger than
+    L2): the time per call and its bandwidth over the algorithmic bytes, each sweep reading and
+    writing the raster once (restrict and prolongation read one raster and write the other)."""
+    import torch
+
+    from deeptime_gpu import _lib as L
+
+    w, h, cells = GRID_W, GRID_H, GRID_W * GRID_H
+    rng = np.random.default_rng(17)
+    fine = torch.from_numpy(rng.standard_normal((h, w))).cuda()
+    other = torch.empty_like(fine)
+    coarse = torch.empty((h // 2, w // 2), dtype=torch.float64, device="cuda")
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def P(t):
+        return ctypes.c_void_p(t.data_ptr())
+
+    cases = {
+        "restrict_by_2": (lambda: lib.dt_grid_restrict_dev(w, h, 2, P(fine), P(coarse), sp), 8 * cells * 1.25),
+        "prolong_linear_2": (lambda: lib.dt_grid_prolong_linear_dev(w // 2, h // 2, 2, P(coarse), P(other), sp),
+                             8 * cells * 1.25),
+        "prolong_const_2": (lambda: lib.dt_grid_prolong_const_dev(w // 2, h // 2, 2, P(coarse), P(other), sp),
+                            8 * cells * 1.25),
+        "binomial_1_pass": (lambda: lib.dt_grid_binomial_dev(w, h, 1, P(fine), P(other), sp), 2 * 16 * cells),
+        "box_blur_r2_2_passes": (lambda: lib.dt_grid_box_blur_dev(w, h, 1, 2, 2, P(fine), P(other), sp), 4 * 16 * cells),
+    }
+    out = {"raster": f"{w}x{h} FP64 ({8 * cells / 1e6:.0f} MB), the time per call, L2 not flushed (the raster is larger)"}
+    for name, (fn, nbytes) in cases.items():
+        L.check(fn())
+        ms, _ = timed(lambda i: L.check(fn()), steps)
+        ms = max_over_ranks(ms, world) / steps
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        out[name] = {"ms": ms, "algorithmic_bytes": nbytes, "GB/s": gbs, "frac_of_hbm_peak": gbs / peak}
+    return out
+
+
+def cube_leg(lib, stream, timed, max_over_ranks, world, steps, problem):
+    """The cube grid's implicit diffusion (surface/cube/diffusion.rs::solve, the multigrid
+    solver): 6 x 256^2 = 393 216 cells, the package's seeded geometry (cube.topology and
+    inputs.cube_problem), RMS tolerance 1e-6 m, dt 7 and 60. Device time per solve with the
+    fields resident (each step restores h on the stream first, 3 MB), and end to end through
+    dt_cube_diff_solve from host arrays."""
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import cube as C
+
+    slots, lap, areas, kd, h0 = problem
+    cd = C.CubeDiffusion(CUBE_N, slots, lap, areas)
+    L.check(lib.dt_cube_set_stream(cd._h, ctypes.c_void_p(stream.cuda_stream)))
+    kd_d, h0_d = torch.from_numpy(kd).cuda(), torch.from_numpy(h0).cuda()
+    x_d = torch.empty_like(h0_d)
+    x_h = [torch.from_numpy(h0.copy()).pin_memory() for _ in range(steps + 1)]
+
+    def dev(dt):
+        with torch.cuda.stream(stream):
+            x_d.copy_(h0_d)
+        rep = L.Report()
+        L.check(lib.dt_cube_diff_solve_dev(cd._h, ctypes.c_void_p(x_d.data_ptr()), ctypes.c_void_p(kd_d.data_ptr()),
+                                           ctypes.c_double(dt), ctypes.c_double(CUBE_TOL_M), ctypes.byref(rep)))
+        return rep
+
+    def host(dt, k):
+        # a fresh pinned copy of h per call: the solve overwrites h in place
+        rep = L.Report()
+        L.check(lib.dt_cube_diff_solve(cd._h, ctypes.c_void_p(x_h[k].data_ptr()), ctypes.c_void_p(kd.ctypes.data),
+                                       ctypes.c_double(dt), ctypes.c_double(CUBE_TOL_M), ctypes.byref(rep)))
+        return rep
+
+    out = {"workload": f"cube-grid implicit diffusion, 6x{CUBE_N}^2 cells, FP64 CG + FP32 damped-Jacobi V-cycle, "
+                       f"RMS tolerance {CUBE_TOL_M:g} m", "levels": cd.levels}
+    for dt in CUBE_DTS:
+        dev(dt)
+        ms, reps = timed(lambda i: dev(dt), steps)
+        for t in x_h:
+            t.copy_(torch.from_numpy(h0))
+        host(dt, steps)
+        ems, _ = timed(lambda i: host(dt, i), steps)
+        out[f"dt_{dt:g}"] = {"ms_per_solve": max_over_ranks(ms, world) / steps,
+                             "e2e_ms_per_solve": max_over_ranks(ems, world) / steps,
+                             "iterations": statistics.mean(r.iterations for r in reps),
+                             "rms_residual_m": max(r.error_m for r in reps)}
+    cd.close()
+    return out
+
+
+def cube_problem():
+    from deeptime_gpu import cube as C
+    from deeptime_gpu import inputs as I
+
+    slots = C.topology(CUBE_N)
+    return (slots,) + tuple(I.cube_problem(CUBE_N, 5, slots))
+
+
+def oracle_cube_ms(problem):
+    """The oracle's time per cube solve at each dt, one solve each."""
+    from oracle import oracle as O
+
+    slots, lap, areas, kd, h0 = problem
+    out = {}
+    for dt in CUBE_DTS:
+        t = time.perf_counter()
+        _, its = O.cube_diff_solve(CUBE_N, slots, lap, areas, kd, dt, CUBE_TOL_M, h0)
+        out[f"dt_{dt:g}"] = {"ms_per_solve": (time.perf_counter() - t) * 1e3, "iterations": its}
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -464,6 +582,11 @@ def main():
     }
     if not args.no_diffusion:
         line["diffusion"] = diffusion_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4))
+    cube_case = None
+    if not args.no_helpers:
+        line["grid_helpers"] = grid_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4), peak)
+        cube_case = cube_problem()
+        line["cube"] = cube_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4), cube_case)
     step_sets = None
     if not args.no_step_raster:
         step_sets = step_inputs()
@@ -480,6 +603,9 @@ def main():
                 "ms_per_solve": secs * 1e3, "iterations": its,
                 "sample": f"the oracle's solve of the step raster's call on each of its {len(step_sets)} input sets, "
                           f"setup included, OpenMP on all {os.cpu_count()} host threads"}
+        if cube_case is not None:
+            line["cpu_baseline"]["cube"] = dict(oracle_cube_ms(cube_case), sample=(
+                f"the oracle's cube solve, one at each dt, OpenMP on all {os.cpu_count()} host threads"))
     if rank == 0:
         print(json.dumps(line), flush=True)
     sv.close()

@@ -123,3 +123,24 @@ def diffusion_problem(w: int, h: int, sigma: float, seed: int, topo_std: float =
     v = (v - lo) / (hi - lo) if hi > lo else np.zeros_like(v)
     s = 10.0 ** (-1.0 + 3.0 * v)
     return topo, s
+
+
+def cube_problem(n: int, seed: int, slots: np.ndarray):
+    """(lap, areas, kd, h) for the cube grid's diffusion on `slots` (cube.topology(n)): cell
+    areas within 20% of each other; coupling weights symmetric across every pair, as
+    CubeGrid::lap is (each pair takes the value its lower-indexed cell computed,
+    sphere/cube.rs:300-316), side pairs near 1 and diagonal pairs small; a diffusivity field with
+    a sharp land-sea edge; h of std 1000 m. Seeded by numpy's default generator."""
+    rng = np.random.default_rng(seed)
+    cells = 6 * n * n
+    areas = 1.0 + 0.2 * rng.random(cells)
+    raw = np.where(np.arange(8) % 2 == 0, 0.8 + 0.4 * rng.random((cells, 8)), 0.05 + 0.15 * rng.random((cells, 8)))
+    valid = slots != 0xFFFFFFFF
+    m = np.where(valid, slots, 0).astype(np.int64)
+    c = np.arange(cells)[:, None]
+    back = np.argmax(slots[m] == c[:, :, None], axis=2)  # the slot of c in its neighbour m's table
+    lap = np.where(m > c, raw, raw[m, back])
+    lap = np.where(valid, lap, 0.0)
+    kd = np.where(rng.random(cells) < 0.3, 0.02, 1.0) * (0.5 + rng.random(cells))
+    h = 1000.0 * rng.standard_normal(cells)
+    return lap, areas, kd, h

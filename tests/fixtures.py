@@ -67,20 +67,9 @@ SIZES = [(1, 1), (1, 7), (7, 1), (2, 2), (2, 5), (3, 5), (5, 3), (17, 9), (33, 3
 
 
 def cube_case(n, seed, slots):
-    """A seeded cube-grid geometry for the cube diffusion's parity tests: cell areas within 20% of
-    each other and coupling weights symmetric across every pair (as CubeGrid::lap is: each pair
-    takes the value its lower-indexed cell computed, sphere/cube.rs:300-316), side pairs near 1,
-    diagonal pairs small, plus a diffusivity field with a sharp land-sea edge."""
-    rng = np.random.default_rng(seed)
-    cells = 6 * n * n
-    areas = 1.0 + 0.2 * rng.random(cells)
-    raw = np.where(np.arange(8) % 2 == 0, 0.8 + 0.4 * rng.random((cells, 8)), 0.05 + 0.15 * rng.random((cells, 8)))
-    valid = slots != 0xFFFFFFFF
-    m = np.where(valid, slots, 0).astype(np.int64)
-    c = np.arange(cells)[:, None]
-    km = np.argmax(slots[m] == c[:, :, None], axis=2)  # the slot of c in its neighbour m's table
-    lap = np.where(m > c, raw, raw[m, km])
-    lap = np.where(valid, lap, 0.0)
-    kd = np.where(rng.random(cells) < 0.3, 0.02, 1.0) * (0.5 + rng.random(cells))
-    h = 1000.0 * rng.standard_normal(cells)
-    return lap, areas, kd, h
+    """A seeded cube-grid geometry for the cube diffusion's parity tests (the package's
+    inputs.cube_problem): cell areas within 20% of each other, symmetric coupling weights (side
+    pairs near 1, diagonal pairs small), a diffusivity field with a sharp land-sea edge."""
+    from deeptime_gpu import inputs as I
+
+    return I.cube_problem(n, seed, slots)

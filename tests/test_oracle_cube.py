@@ -31,6 +31,14 @@ def test_the_topology_is_mutual_and_misses_one_diagonal_at_each_cube_corner(n):
     assert int((s == NO).sum()) == 6 * 4
 
 
+@pytest.mark.parametrize("n", [1, 2, 3, 8, 15, 64])
+def test_the_packages_topology_is_the_oracles(n):
+    # the slots a caller builds with the package (deeptime_gpu.cube.topology) are the oracle's
+    from deeptime_gpu import cube as C
+
+    assert np.array_equal(C.topology(n), O.cube_topology(n))
+
+
 def test_the_operator_is_symmetric():
     n = 8
     s = O.cube_topology(n)
