@@ -61,9 +61,10 @@ def test_binomial_is_the_references(w, h, passes):
 
 
 @pytest.mark.parametrize("w,h", SIZES)
-@pytest.mark.parametrize("r,passes", [(1, 2), (2, 2), (3, 1), (0, 2)])
+@pytest.mark.parametrize("r,passes", [(1, 2), (2, 2), (3, 1), (0, 2), (31, 1), (40, 1), (63, 1), (70, 1)])
 @pytest.mark.parametrize("wrap", [True, False])
 def test_box_blur_is_the_references(w, h, r, passes, wrap):
+    # r up to 31 and up to 63: the line kernel's two window widths; 70: the plain kernels
     rng = np.random.default_rng(w + 11 * h + r)
     v = rng.standard_normal((h, w)) * 50.0 + 25.0
     t, s = dev(v), torch.empty((h, w), dtype=torch.float64, device="cuda")
