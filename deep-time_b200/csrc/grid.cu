@@ -42,30 +42,62 @@ __global__ void k_restrict(int w, int ws, int hs, int f, double norm, const doub
 
 // The 2-D element-wise grids: blockIdx.x * blockDim.x + threadIdx.x is the column, rows go
 // blockIdx.y, blockIdx.y + gridDim.y, ...
+// V = 2: a thread takes columns 2c and 2c + 1 and stores them as one 16-byte word (the caller
+// checks that rows start on 16 bytes: w even, out aligned)
+template <int V>
 __global__ void k_prolong_const(int ws, int hs, int f, const double* __restrict__ v, double* __restrict__ out) {
   const int w = ws * f, h = hs * f;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = V * (blockIdx.x * blockDim.x + threadIdx.x);
   if (i >= w) return;
-  const int ci = i / f;
+  if constexpr (V == 2) {
+    const int c0 = i / f, c1 = (i + 1) / f;
 #pragma unroll 4
-  for (int j = blockIdx.y; j < h; j += gridDim.y) out[(size_t)j * w + i] = v[(size_t)(j / f) * ws + ci];
+    for (int j = blockIdx.y; j < h; j += gridDim.y) {
+      const double* row = v + (size_t)(j / f) * ws;
+      *reinterpret_cast<double2*>(out + (size_t)j * w + i) = make_double2(row[c0], row[c1]);
+    }
+  } else {
+    const int ci = i / f;
+#pragma unroll 4
+    for (int j = blockIdx.y; j < h; j += gridDim.y) out[(size_t)j * w + i] = v[(size_t)(j / f) * ws + ci];
+  }
+}
+
+// The column's share of prolong_linear (the same for every row): the two coarse columns and the
+// weights of the bilinear blend
+struct XShare {
+  int i0, i1;
+  double tx, ux;
+};
+__device__ __forceinline__ XShare x_share(int i, int ws, double fd) {
+  const double x = __dsub_rn(__ddiv_rn(__dadd_rn((double)i, 0.5), fd), 0.5);
+  const double x0 = floor(x);
+  XShare s;
+  s.tx = __dsub_rn(x, x0);
+  s.ux = __dsub_rn(1.0, s.tx);
+  long long iw = (long long)x0 % ws;
+  s.i0 = (int)(iw < 0 ? iw + ws : iw);
+  s.i1 = (s.i0 + 1) % ws;
+  return s;
+}
+__device__ __forceinline__ double bilinear(const double* r0, const double* r1, const XShare& s, double ty, double uy) {
+  const double a = __dadd_rn(__dmul_rn(r0[s.i0], s.ux), __dmul_rn(r0[s.i1], s.tx));
+  const double b = __dadd_rn(__dmul_rn(r1[s.i0], s.ux), __dmul_rn(r1[s.i1], s.tx));
+  return __dadd_rn(__dmul_rn(a, uy), __dmul_rn(b, ty));
 }
 
 // 256 threads a block: the rows' shares (y, its floor and weight) are computed once per row, by
-// one thread each, into shared memory, 256 rows at a time
+// one thread each, into shared memory, 256 rows at a time. V as in k_prolong_const.
+template <int V>
 __global__ void __launch_bounds__(256) k_prolong_linear(int ws, int hs, int f, const double* __restrict__ v,
                                                         double* __restrict__ out) {
   __shared__ double s_ty[256];
   __shared__ int s_j0[256];
   const int w = ws * f, h = hs * f;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = V * (blockIdx.x * blockDim.x + threadIdx.x);
   const double fd = (double)f, top = (double)(hs - 1);
-  // the column's share, the same for every row
-  const double x = __dsub_rn(__ddiv_rn(__dadd_rn((double)min(i, w - 1), 0.5), fd), 0.5);
-  const double x0 = floor(x);
-  const double tx = __dsub_rn(x, x0), ux = __dsub_rn(1.0, tx);
-  long long iw = (long long)x0 % ws;
-  const int i0 = (int)(iw < 0 ? iw + ws : iw), i1 = (i0 + 1) % ws;
+  const XShare sx0 = x_share(min(i, w - 1), ws, fd);
+  const XShare sx1 = x_share(min(i + V - 1, w - 1), ws, fd);
   const int step = gridDim.y;
   for (int base = blockIdx.y; base < h; base += 256 * step) {
     const int jr = base + threadIdx.x * step;
@@ -85,9 +117,12 @@ __global__ void __launch_bounds__(256) k_prolong_linear(int ws, int hs, int f, c
         const int j0 = s_j0[q], j1 = min(j0 + 1, hs - 1);
         const double* r0 = v + (size_t)j0 * ws;
         const double* r1 = v + (size_t)j1 * ws;
-        const double a = __dadd_rn(__dmul_rn(r0[i0], ux), __dmul_rn(r0[i1], tx));
-        const double b = __dadd_rn(__dmul_rn(r1[i0], ux), __dmul_rn(r1[i1], tx));
-        out[(size_t)j * w + i] = __dadd_rn(__dmul_rn(a, uy), __dmul_rn(b, ty));
+        if constexpr (V == 2) {
+          *reinterpret_cast<double2*>(out + (size_t)j * w + i) =
+              make_double2(bilinear(r0, r1, sx0, ty, uy), bilinear(r0, r1, sx1, ty, uy));
+        } else {
+          out[(size_t)j * w + i] = bilinear(r0, r1, sx0, ty, uy);
+        }
       }
     }
     __syncthreads();
@@ -367,6 +402,9 @@ static dim3 grid2d(int w, int h) {
   return dim3(gx, std::min(gy, 65535u));
 }
 
+// Column pairs as 16-byte stores: every row must start on 16 bytes
+static bool prolong_pairs(int w, const double* out) { return (w % 2) == 0 && ((uintptr_t)out % 16) == 0; }
+
 // The box blur's line kernel for one direction: false when r is too wide for its ring.
 template <bool ROWS>
 static bool launch_blur_lines(int w, int h, int r, bool wrap, double norm, const double* v, double* out, cudaStream_t st) {
@@ -409,7 +447,11 @@ dt_status dt_grid_prolong_const_dev(int ws, int hs, int f, const double* coarse,
     set_error("dt_grid_prolong_const_dev: bad arguments (ws %d, hs %d, f %d)", ws, hs, f);
     return DT_BAD_ARG;
   }
-  k_prolong_const<<<grid2d(ws * f, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  if (prolong_pairs(ws * f, fine)) {
+    k_prolong_const<2><<<grid2d((ws * f) / 2, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  } else {
+    k_prolong_const<1><<<grid2d(ws * f, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  }
   DT_CUDA(cudaGetLastError());
   return DT_OK;
 }
@@ -424,7 +466,11 @@ dt_status dt_grid_prolong_linear_dev(int ws, int hs, int f, const double* coarse
     DT_CUDA(cudaMemcpyAsync(fine, coarse, n * sizeof(double), cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
     return DT_OK;
   }
-  k_prolong_linear<<<grid2d(ws * f, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  if (prolong_pairs(ws * f, fine)) {
+    k_prolong_linear<2><<<grid2d((ws * f) / 2, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  } else {
+    k_prolong_linear<1><<<grid2d(ws * f, hs * f), 256, 0, (cudaStream_t)stream>>>(ws, hs, f, coarse, fine);
+  }
   DT_CUDA(cudaGetLastError());
   return DT_OK;
 }
