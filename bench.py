@@ -18,6 +18,7 @@ throughput over the max-over-ranks device time.
   roofline  the dominant kernel's algorithmic bytes per launch / its event-timed launch duration
   cpu_baseline  the oracle (a C++ restatement of the reference's CPU solver, FP64, its own
             3-level bank preconditioner) on the host's cores, a bounded sample extrapolated
+  sphere    the same solve on the sphere's row metric (a band of latitudes +-58 degrees)
   step_raster  the timestep's own call at 1024 x 328 (39 km cells, max|z| < 2 m, at most 60
             iterations), FP64, device and end to end; the oracle's time for the same
             call sits in cpu_baseline
@@ -70,6 +71,7 @@ def parse():
     ap.add_argument("--no-diffusion", action="store_true", help="skip the diffusion solve's leg")
     ap.add_argument("--no-helpers", action="store_true",
                     help="skip the legs of the step's grid helpers and the cube grid's diffusion")
+    ap.add_argument("--no-sphere", action="store_true", help="skip the sphere row metric's leg")
     ap.add_argument("--no-step-raster", action="store_true",
                     help="skip the timestep raster's leg (1024 x 328, the reference's max|z| rule)")
     ap.add_argument("--warm", default="unet" if os.path.exists(WEIGHTS) else "none", choices=["unet", "none"],
@@ -271,6 +273,47 @@ def step_raster_leg(lib, stream, timed, max_over_ranks, world, steps, sets):
                      "iterations": statistics.mean(r.iterations for r in reps),
                      "converged": all(r.converged for r in reps),
                      "max_error_m": max(r.error_m for r in reps)}
+    sv.close()
+    return out
+
+
+SPHERE_SIN = 0.85  # the band's edge: sin(58.2 degrees)
+
+
+def sphere_leg(lib, stream, timed, max_over_ranks, world, steps, dev, fp, precond):
+    """The headline's solve on the sphere's row metric (RowMetric::from_sin_faces, Solver::with_metric):
+    the same 4096 x 2048 inputs, rows of equal area between latitudes +-58.2 degrees (sines of
+    latitude at the row faces from 0.85 to -0.85), to relative residual 1e-8 with the reference
+    preconditioner, FP64 and FP32 with FP64 reliable updates, from x = 0. The operator takes the
+    rows' couplings and the spectral pass solves each wavenumber's pentadiagonal system along y."""
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import flexure as F
+
+    r_m = 0.5 * H * DX / SPHERE_SIN
+    faces = np.clip((0.5 * H - np.arange(H + 1)) * DX / r_m, -1.0, 1.0)
+    sv = F.Solver(W, H, DX, F.row_metric_from_sin_faces(faces))
+    L.check(lib.dt_flex_set_stream(sv._h, ctypes.c_void_p(stream.cuda_stream)))
+    x = torch.zeros((H, W), dtype=torch.float64, device="cuda")
+
+    def solve(i, p):
+        d, c, b = dev[i % len(dev)]
+        rep = L.Report()
+        L.check(lib.dt_flex_solve_dev(sv._h, ctypes.c_void_p(d.data_ptr()), ctypes.c_void_p(c.data_ptr()),
+                                      ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(x.data_ptr()), ctypes.byref(p),
+                                      ctypes.byref(rep)))
+        return rep
+
+    out = {"workload": f"the headline's {W}x{H} solve on the row metric, equal-area rows between sin(latitude) "
+                       f"+-{SPHERE_SIN}, rel. residual {TOL:g}, reference preconditioner, x = 0"}
+    for name, prec in (("fp64", L.PREC_FP64), ("mixed_reliable", L.PREC_MIXED_RELIABLE)):
+        p = fp(prec, precond)
+        solve(0, p)
+        ms, reps = timed(lambda i: solve(i, p), steps)
+        out[name] = {"ms_per_solve": max_over_ranks(ms, world) / steps,
+                     "iterations": statistics.mean(r.iterations for r in reps),
+                     "rel_residual": max(r.rel_residual for r in reps)}
     sv.close()
     return out
 
@@ -582,6 +625,8 @@ def main():
     }
     if not args.no_diffusion:
         line["diffusion"] = diffusion_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4))
+    if not args.no_sphere:
+        line["sphere"] = sphere_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 2), dev, fp, precond)
     cube_case = None
     if not args.no_helpers:
         line["grid_helpers"] = grid_leg(lib, stream, timed, max_over_ranks, world, min(args.steps, 4), peak)

@@ -43,6 +43,25 @@ def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
+def row_metric_from_sin_faces(sin_faces, f: int = 1):
+    """RowMetric::from_sin_faces (flexure.rs:977-1000): the sphere's row metric of a raster whose
+    row boundaries sit at the sines of latitude `sin_faces` (h f + 1 of them, every f-th taken).
+    a_j = 1 / max(1 - m_j^2, least) with m_j the mean of row j's two faces and least half the
+    largest step between faces (at least 1e-12); b_k = 1 - s_k^2 inside, 0 at the raster's edges.
+    Returns (a, b) for Solver(w, h, dx, (a, b))."""
+    f = max(int(f), 1)
+    s = np.clip(_f64(sin_faces)[::f], -1.0, 1.0)
+    h = (len(sin_faces) - 1) // f
+    s = s[: h + 1]
+    full = float(np.max(np.abs(np.diff(s)))) if h > 0 else 0.0
+    least = max(0.5 * full, 1e-12)
+    m = 0.5 * (s[:-1] + s[1:])
+    a = 1.0 / np.maximum(1.0 - m * m, least)
+    b = 1.0 - s * s
+    b[0] = b[-1] = 0.0
+    return a, b
+
+
 def params(precond=L.PRECOND_REFERENCE, stop=L.STOP_MAX_Z, precision=L.PREC_FP64, warm_start=L.WARM_NONE, tol=2.0,
            max_iterations=60, inner_tol=1e-5, max_refinements=8, host_loop=0) -> L.FlexParams:
     p = L.FlexParams()

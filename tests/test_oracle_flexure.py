@@ -196,6 +196,19 @@ def sphere_faces(h, dx, r_m):
     return np.clip((0.5 * h - k) * dx / r_m, -1.0, 1.0)
 
 
+@pytest.mark.parametrize("h,f,r_frac", [(164, 1, 0.5), (41, 1, 0.3), (300, 2, 1.0), (2048, 1, 0.59)])
+def test_the_packages_row_metric_is_the_oracles(h, f, r_frac):
+    # the metric a caller builds with the package (deeptime_gpu.flexure.row_metric_from_sin_faces),
+    # bit for bit, on rasters that reach the poles (r_frac <= 0.5) and bands that do not
+    from deeptime_gpu import flexure as F
+
+    dx = 10_000.0
+    faces = sphere_faces(h * f, dx, r_frac * h * f * dx)
+    a, b = F.row_metric_from_sin_faces(faces, f)
+    ao, bo = O.row_metric_from_sin_faces(faces, f)
+    assert np.array_equal(a, ao) and np.array_equal(b, bo)
+
+
 def test_the_row_metric_is_the_block_metric_at_the_equator():
     # flexure.rs:5351-5381
     w, h = 512, 164
