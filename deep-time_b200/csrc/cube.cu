@@ -45,6 +45,8 @@ constexpr size_t CUBE_COARSEST = 64;   // multigrid.rs:54
 constexpr int CUBE_COARSE_SWEEPS = 16; // multigrid.rs:56
 constexpr int CUBE_CG_MAX_ITER = 400;  // surface/diffusion.rs:497
 constexpr int CUBE_RED_BLOCKS = 592;   // partial sums per reduction (4 per SM)
+constexpr size_t CUBE_FUSE_CELLS = 1536;  // levels this small run their part of the cycle in one block
+constexpr int CUBE_MAX_FUSED = 24;        // levels one fused launch carries
 
 // ---- the operator ----
 __global__ void k_cube_couplings(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ lap,
@@ -374,6 +376,75 @@ __global__ void k_to_f64(size_t n, const float* __restrict__ a, double* __restri
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) b[i] = (double)a[i];
 }
 
+// The coarse levels' part of the V-cycle in one block of 1024 threads: the launches of those
+// levels (sweeps, residual, restriction, the coarsest level's sweeps, prolongation) in the same
+// order and with the same arithmetic per cell, a block barrier where a launch ended. The vectors
+// written here are read through plain pointers (not the read-only path), so that every phase sees
+// the last one's writes.
+struct MgLevelDev {
+  unsigned cells;
+  const uint32_t *ptr, *col, *kid_ptr, *kids, *parent;
+  const float *val, *diag;
+  float *r, *z, *t;
+};
+struct MgCoarse {
+  int count;  // levels carried; the last is the coarsest
+  MgLevelDev lv[CUBE_MAX_FUSED];
+};
+
+__device__ __forceinline__ float mg_az_plain(unsigned i, const MgLevelDev& L, const float* z) {
+  float az = __fmul_rn(L.diag[i], z[i]);
+  for (uint32_t e = L.ptr[i]; e < L.ptr[i + 1]; ++e) az = __fsub_rn(az, __fmul_rn(L.val[e], z[L.col[e]]));
+  return az;
+}
+
+__global__ void __launch_bounds__(1024) k_mg_coarse_cycle(MgCoarse m) {
+  float* z[CUBE_MAX_FUSED];
+  float* t[CUBE_MAX_FUSED];
+  for (int l = 0; l < m.count; ++l) {
+    z[l] = m.lv[l].z;
+    t[l] = m.lv[l].t;
+  }
+  const unsigned tid = threadIdx.x, nt = blockDim.x;
+  auto sweep = [&](int l, bool first) {
+    const MgLevelDev& L = m.lv[l];
+    if (first) {
+      for (unsigned i = tid; i < L.cells; i += nt) z[l][i] = __fdiv_rn(__fmul_rn(CUBE_OMEGA, L.r[i]), L.diag[i]);
+    } else {
+      for (unsigned i = tid; i < L.cells; i += nt) {
+        const float az = mg_az_plain(i, L, z[l]);
+        t[l][i] = __fadd_rn(z[l][i], __fdiv_rn(__fmul_rn(CUBE_OMEGA, __fsub_rn(L.r[i], az)), L.diag[i]));
+      }
+      float* q = z[l];
+      z[l] = t[l];
+      t[l] = q;
+    }
+    __syncthreads();
+  };
+  const int last = m.count - 1;
+  for (int l = 0; l < last; ++l) {
+    for (int k = 0; k < CUBE_NU; ++k) sweep(l, k == 0);
+    const MgLevelDev& L = m.lv[l];
+    for (unsigned i = tid; i < L.cells; i += nt) t[l][i] = __fsub_rn(L.r[i], mg_az_plain(i, L, z[l]));
+    __syncthreads();
+    const MgLevelDev& C = m.lv[l + 1];
+    for (unsigned q = tid; q < C.cells; q += nt) {
+      float sum = 0.f;
+      for (uint32_t e = C.kid_ptr[q]; e < C.kid_ptr[q + 1]; ++e) sum = __fadd_rn(sum, t[l][C.kids[e]]);
+      C.r[q] = sum;
+    }
+    __syncthreads();
+  }
+  for (int k = 0; k < CUBE_COARSE_SWEEPS; ++k) sweep(last, k == 0);
+  for (int l = last - 1; l >= 0; --l) {
+    const MgLevelDev& L = m.lv[l];
+    const MgLevelDev& C = m.lv[l + 1];
+    for (unsigned c = tid; c < L.cells; c += nt) z[l][c] = __fadd_rn(z[l][c], z[l + 1][C.parent[c]]);
+    __syncthreads();
+    for (int k = 0; k < CUBE_NU; ++k) sweep(l, false);
+  }
+}
+
 // alpha = rz / pap; beta = rz_new / rz, rz = rz_new (the CG scalars, on the device)
 // alpha = rz / pap, or the breakdown flag (pap not positive, or NaN: diffusion.rs:444-446)
 __global__ void k_cube_alpha(const double* __restrict__ rz, const double* __restrict__ pap, double* __restrict__ alpha,
@@ -567,9 +638,30 @@ void cube_sweep(dt_cube* s, CubeLevel& lv, bool first) {
   std::swap(lv.z, lv.t);
 }
 
+// The cycle from level l0 down in one block (k_mg_coarse_cycle). The host's view of each level's
+// z and t then takes the swaps the replaced launches make: NU - 1 + NU on a level with a coarser
+// one below, COARSE_SWEEPS - 1 on the coarsest.
+void cube_coarse_cycle(dt_cube* s, size_t l0) {
+  MgCoarse m{};
+  m.count = (int)(s->levels.size() - l0);
+  for (int i = 0; i < m.count; ++i) {
+    const CubeLevel& lv = s->levels[l0 + i];
+    m.lv[i] = MgLevelDev{(unsigned)lv.cells, lv.ptr, lv.col, lv.kid_ptr, lv.kids, lv.parent, lv.val, lv.diag, lv.r, lv.z, lv.t};
+  }
+  k_mg_coarse_cycle<<<1, 1024, 0, s->stream>>>(m);
+  for (size_t l = l0; l < s->levels.size(); ++l) {
+    const int swaps = l + 1 == s->levels.size() ? CUBE_COARSE_SWEEPS - 1 : 2 * CUBE_NU - 1;
+    if (swaps & 1) std::swap(s->levels[l].z, s->levels[l].t);
+  }
+}
+
 // multigrid.rs:312-363
 void cube_vcycle(dt_cube* s, size_t l) {
   CubeLevel& lv = s->levels[l];
+  if (lv.cells <= CUBE_FUSE_CELLS && s->levels.size() - l <= (size_t)CUBE_MAX_FUSED) {
+    cube_coarse_cycle(s, l);
+    return;
+  }
   if (l + 1 == s->levels.size()) {
     for (int k = 0; k < CUBE_COARSE_SWEEPS; ++k) cube_sweep(s, lv, k == 0);
     return;
