@@ -17,7 +17,8 @@ throughput over the max-over-ranks device time.
             the D2H copy of x are inside the timed region
   roofline  the dominant kernel's algorithmic bytes per launch / its event-timed launch duration
   cpu_baseline  the oracle (a C++ restatement of the reference's CPU solver, FP64, its own
-            3-level bank preconditioner) on the host's cores, a bounded sample extrapolated
+            3-level bank preconditioner) on the host's cores: complete solves to 1e-8 timed by
+            the wall clock, on all host threads and on 8 (the reference's own bench setting)
   sphere    the same solve on the sphere's row metric (a band of latitudes +-58 degrees)
   step_raster  the timestep's own call at 1024 x 328 (39 km cells, max|z| < 2 m, at most 60
             iterations), FP64, device and end to end; the oracle's time for the same
@@ -26,7 +27,11 @@ throughput over the max-over-ranks device time.
             each call's bandwidth over its algorithmic bytes
   cube      the cube grid's diffusion at 6 x 256^2 cells, device and end to end; the oracle's
             time beside it in cpu_baseline
---impl reference times that CPU restatement alone, as the reference arm.
+--impl reference times that CPU restatement alone, as the reference arm: complete solves of the
+same input sets, one per step, after the warm-up solves.
+
+Run as `python bench.py --gpus N` without torchrun's environment, it launches its own N ranks
+(torch.distributed.run on 127.0.0.1) and rank 0 prints the line.
 """
 from __future__ import annotations
 
@@ -48,11 +53,27 @@ import numpy as np  # noqa: E402
 
 W, H, DX, SIGMA = 4096, 2048, 2500.0, 32.0
 TOL = 1e-8
+REF_THREADS = 8  # the reference's own benchmark runs its solver pool on 8 threads
 KERNEL_NAMES = ["flex_apply", "cg_update", "cg_direction", "fft_rows_fwd", "dct_cols_divide_idct", "fft_rows_inv_dot",
                 "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_bank"]
 WEIGHTS = os.path.join(ROOT, "deep-time_b200", "weights", "unet_flexure.bin")
 MODEL_DX = 10_000.0  # the U-Net's cell size: trained on 512 x 256 rasters of 10 km
 METRIC = "flexure solves/s to relative residual 1e-8 @4096x2048 (time-to-1e-8 per solve = 1000/value ms)"
+
+
+def set_raster(spec):
+    """--raster W,H,DX_M,SIGMA: another raster for a quick check (the default is the 4096 x 2048 workload)."""
+    global W, H, DX, SIGMA, METRIC
+    w, h, dx, sg = spec.split(",")
+    W, H, DX, SIGMA = int(w), int(h), float(dx), float(sg)
+    METRIC = f"flexure solves/s to relative residual 1e-8 @{W}x{H} (time-to-1e-8 per solve = 1000/value ms)"
+
+
+def workload_config(n_inputs):
+    """The `config` both arms print: the workload alone, so that the two lines compare like for like."""
+    return {"workload": f"flexure PCG to rel. residual {TOL:g}, {W}x{H}, dx {DX / 1e3:g} km, sigma {SIGMA:g} cells",
+            "inputs": f"{n_inputs} seeded input sets cycled, {3 * W * H * 8 / 1e6:.0f} MB each: " +
+                      ("larger than L2, no flush" if 3 * W * H * 8 > 126e6 else "smaller than L2 (a quick check)")}
 
 
 def parse():
@@ -62,6 +83,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
+    ap.add_argument("--raster", default=None, help="W,H,DX_M,SIGMA: another flexure raster for a quick check")
     ap.add_argument("--precond", default="reference", choices=["reference", "mean_d"])
     ap.add_argument("--precision", default="reliable", choices=["reliable", "refinement"],
                     help="mixed precision of the benchmarked solve: one FP32 PCG with FP64 reliable updates, or FP32 "
@@ -188,28 +210,35 @@ def make_inputs(k, seed0=1000):
     return [I.flexure_problem(W, H, SIGMA, seed0 + 100 * i) for i in range(k)]
 
 
-def oracle_cpu_baseline(d, c, b, its_needed, max_seconds=30.0):
-    """The oracle's FP64 solve (the reference's preconditioner) at full size: setup and per-iteration
-    time from runs capped at 1 and 3 iterations, extrapolated to the iterations the same algorithm
-    needs to reach 1e-8 (its_needed)."""
+def oracle_full_solve_seconds(d, c, b):
+    """Wall-clock seconds of one complete oracle solve to relative residual 1e-8 (FP64 PCG with the
+    reference's 3-level bank + Jacobi preconditioner, from x = 0), and its iteration count."""
     from oracle import oracle as O
 
-    def timed(its):
-        t = time.perf_counter()
-        O.flex_solve(d, c, b, DX, TOL, its, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
-        return time.perf_counter() - t
+    t = time.perf_counter()
+    _, rep = O.flex_solve(d, c, b, DX, TOL, 20000, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
+    return time.perf_counter() - t, rep["iterations"]
 
-    t1 = timed(1)
-    t3 = timed(3)
-    per_it = max((t3 - t1) / 2.0, 1e-9)
-    setup = max(t1 - per_it, 0.0)
-    seconds = setup + per_it * its_needed
-    return {"value": 1.0 / seconds, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-            "sample": (f"oracle FP64 PCG with the reference's 3-level bank + Jacobi preconditioner on {W}x{H}: "
-                       f"setup {setup:.2f} s and {per_it:.2f} s/iteration measured from solves capped at 1 and 3 "
-                       f"iterations, extrapolated to {its_needed} iterations (the count the same algorithm takes to "
-                       f"1e-8 on the GPU); OpenMP on all {os.cpu_count()} host threads"),
-            "seconds_per_solve": seconds}
+
+def oracle_cpu_baseline(inputs, solves=2):
+    """The oracle's complete solves on the host: `solves` of them on all host threads (the median
+    is the value) and one on 8 threads, each timed by the wall clock from x = 0 to 1e-8."""
+    from oracle import oracle as O
+
+    allc = O.set_threads(0)
+    runs = [oracle_full_solve_seconds(*inputs[k % len(inputs)]) for k in range(solves)]
+    secs = [r[0] for r in runs]
+    t8 = O.set_threads(REF_THREADS)
+    s8, it8 = oracle_full_solve_seconds(*inputs[0])
+    O.set_threads(0)
+    med = statistics.median(secs)
+    return {"value": 1.0 / med, "unit": "solves/s", "cores": allc, "kind": "port",
+            "sample": (f"{solves} complete solves of input sets 0..{solves - 1} to {TOL:g} by the oracle (FP64 PCG, the "
+                       f"reference's 3-level bank + Jacobi preconditioner, x = 0), wall clock, OpenMP on all {allc} "
+                       f"host threads; value = 1 / the median"),
+            "seconds_per_solve": secs, "iterations": [r[1] for r in runs],
+            "threads_8": {"value": 1.0 / s8, "seconds_per_solve": s8, "iterations": it8, "threads": t8,
+                          "sample": "one complete solve of input set 0 on 8 host threads (the reference's bench setting)"}}
 
 
 STEP_W, STEP_H, STEP_DX = 1024, 328, 39_000.0
@@ -431,42 +460,53 @@ def oracle_cube_ms(problem):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the oracle (the C++/OpenMP restatement of the reference's flexure::Solver,
+    FP64 with its 3-level bank + Jacobi preconditioner) on all host threads, one complete solve to
+    1e-8 from x = 0 per step over the same input sets as the device arm, after `warmup` untimed
+    solves. Rank 0 alone runs it; the wall clock spans exactly the timed solves."""
     if rank != 0:
         return
     from oracle import oracle as O
 
     O.build() if not os.path.exists(O.LIB_PATH) else None
-    d, c, b = make_inputs(1)[0]
-    # iterations the reference algorithm needs (one full solve, in the warm-up)
-    t = time.perf_counter()
-    x, rep = O.flex_solve(d, c, b, DX, TOL, 2000, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
-    full = time.perf_counter() - t
-    its = rep["iterations"]
-    times = []
-    for k in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        O.flex_solve(d, c, b, DX, TOL, 3, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
-        el = time.perf_counter() - t0
-        if k >= args.warmup:
-            times.append(el)
-    t1 = time.perf_counter()
-    O.flex_solve(d, c, b, DX, TOL, 1, precond=O.PRECOND_REFERENCE, stop=O.STOP_REL_RESIDUAL)
-    one = time.perf_counter() - t1
-    per_it = max((statistics.median(times) - one) / 2.0, 1e-9)
-    seconds = max(one - per_it, 0.0) + per_it * its
-    value = 1.0 / seconds
-    sample = (f"each step: the oracle (C++/OpenMP restatement of the reference's flexure::Solver) solving {W}x{H} capped "
-              f"at 3 iterations; per-iteration time from those steps and a 1-iteration solve, extrapolated to the "
-              f"{its} iterations its full warm-up solve took to 1e-8 ({full:.1f} s measured)")
-    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * seconds, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 fields)", "impl": "reference",
-            "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
-                       "precision": "fp64", "preconditioner": "reference 3-level bank + Jacobi", "iterations": its,
-                       "full_solve_seconds": full},
-            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port", "sample": sample},
+    cores = O.set_threads(0)
+    inputs = make_inputs(max(1, args.inputs))
+    for k in range(args.warmup):
+        oracle_full_solve_seconds(*inputs[k % len(inputs)])
+    secs, its = [], []
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s_k, i_k = oracle_full_solve_seconds(*inputs[k % len(inputs)])
+        secs.append(s_k)
+        its.append(i_k)
+    total = time.perf_counter() - t0
+    value = args.steps / total
+    sample = (f"each step one complete solve of a {W}x{H} input set to {TOL:g} by the oracle (C++/OpenMP restatement of "
+              f"the reference's flexure::Solver, FP64, 3-level bank + Jacobi, x = 0), wall clock, {cores} host threads; "
+              f"{args.steps} timed solves in {total:.1f} s after {args.warmup} warm-up solves")
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded SplitMix64 fields)",
+            "impl": "reference", "config": workload_config(len(inputs)),
+            "method": {"precision": "fp64", "preconditioner": "reference 3-level bank + Jacobi",
+                       "iterations_per_solve": statistics.mean(its),
+                       "seconds_per_solve": {"median": statistics.median(secs), "min": min(secs), "max": max(secs)}},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def launch_ranks(args):
+    """`bench.py --gpus N` outside torchrun: run the same command as N local ranks under
+    torch.distributed.run (127.0.0.1, a free port) and return its exit status."""
+    import socket
+
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -474,6 +514,10 @@ def main():
     if args.case:
         run_case(args.case)
         return
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        raise SystemExit(launch_ranks(args))
+    if args.raster:
+        set_raster(args.raster)
     rank, world, local = dist_init(args.gpus)
     if args.impl == "reference":
         run_reference(args, rank, world)
@@ -579,7 +623,7 @@ def main():
         return rep
 
     solve_host(0)
-    e2e_steps = min(args.steps, 4)
+    e2e_steps = args.steps
     ems, _ = timed(solve_host, e2e_steps)
     ems = max_over_ranks(ems, world)
 
@@ -607,11 +651,10 @@ def main():
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head_ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 inner / f64 refinement", "data": "synthetic (seeded SplitMix64 fields)",
-        "config": {"workload": f"flexure PCG to rel. residual 1e-8, {W}x{H}, dx 2.5 km, sigma 32 cells",
-                   "method": ("mixed precision (one FP32 PCG, FP64 reliable updates of x and r), " if args.precision == "reliable"
-                              else "mixed precision (FP32 inner PCG in FP64 refinement), ") +
-                             f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, {warm_txt}",
-                   "inputs": f"{len(inputs)} seeded input sets cycled, 201 MB each: larger than L2, no flush",
+        "config": workload_config(len(inputs)),
+        "method": {"solve": ("mixed precision (one FP32 PCG, FP64 reliable updates of x and r), " if args.precision == "reliable"
+                             else "mixed precision (FP32 inner PCG in FP64 refinement), ") +
+                            f"{'reference 3-level bank + Jacobi' if levels3 else 'mean-D'} preconditioner, {warm_txt}",
                    "iterations_per_solve": statistics.mean(its), "replicas": world},
         "plain_fp64_gpu": dict(breakdown["plain_fp64_gpu"], speedup_of_value=breakdown["plain_fp64_gpu"]["ms_per_solve"] / head_ms),
         "methods": breakdown,
@@ -639,9 +682,7 @@ def main():
     if rank == 0 and not args.no_accuracy:
         line["accuracy"] = accuracy(lambda p: (solve_dev(0, p), x_dev.cpu().numpy())[1], head, methods, inputs[0])
     if rank == 0 and not args.no_cpu_baseline:
-        d, c, b = inputs[0]
-        ref_its = breakdown["fp64_bank_gpu"]["iterations"]
-        line["cpu_baseline"] = oracle_cpu_baseline(d, c, b, int(round(ref_its)))
+        line["cpu_baseline"] = oracle_cpu_baseline(inputs)
         if step_sets is not None:
             secs, its = oracle_step_seconds(step_sets)
             line["cpu_baseline"]["step_raster"] = {

@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <vector>
 
 #include "common.cuh"
@@ -582,6 +583,10 @@ struct dt_cube {
   // first use.
   cudaGraphExec_t vcycle_exec[2] = {nullptr, nullptr};
   int vcycle_layout = 0;
+  // levels of at most this many cells run their part of the cycle in one block; the environment
+  // variable DT_CUBE_FUSE_CELLS, read at dt_cube_create, overrides it (0: every level launches
+  // its own kernels, the form the fused block reproduces bit for bit)
+  size_t fuse_cells = 0;
 };
 
 namespace {
@@ -658,7 +663,7 @@ void cube_coarse_cycle(dt_cube* s, size_t l0) {
 // multigrid.rs:312-363
 void cube_vcycle(dt_cube* s, size_t l) {
   CubeLevel& lv = s->levels[l];
-  if (lv.cells <= CUBE_FUSE_CELLS && s->levels.size() - l <= (size_t)CUBE_MAX_FUSED) {
+  if (lv.cells <= s->fuse_cells && s->levels.size() - l <= (size_t)CUBE_MAX_FUSED) {
     cube_coarse_cycle(s, l);
     return;
   }
@@ -874,6 +879,8 @@ dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const 
   }
   auto* s = new dt_cube();
   s->n = n;
+  s->fuse_cells = CUBE_FUSE_CELLS;
+  if (const char* e = std::getenv("DT_CUBE_FUSE_CELLS")) s->fuse_cells = std::strtoull(e, nullptr, 10);
   s->cells = cells;
   auto fail = [&](dt_status e) {
     dt_cube_destroy(s);

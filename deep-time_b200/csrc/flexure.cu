@@ -3169,7 +3169,8 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 static std::mutex g_noalloc_lock;
 static double* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
 
-// The scratch's device address on the current device: looked up on the first call per device.
+// The scratch's device address on the current device: looked up on the first call per device and
+// kept for the life of the process (a device reset by the caller leaves it stale).
 static dt_status noalloc_scratch(double** out) {
   int dev = -1;
   DT_CUDA(cudaGetDevice(&dev));
@@ -3203,7 +3204,13 @@ extern "C" dt_status dt_flex_operator_dot_noalloc(int w, int h, double dx, const
     set_error("dt_flex_operator_dot_noalloc: bad raster %d x %d, dx %g", w, h, dx);
     return DT_BAD_ARG;
   }
-  const size_t tiles = (size_t)ceil_div((size_t)w, TBX) * ceil_div((size_t)h, tile_rows<double>());
+  const size_t tile_rows_y = ceil_div((size_t)h, tile_rows<double>());
+  if (tile_rows_y > 65535) {  // the grid's y extent carries the rows of tiles
+    set_error("dt_flex_operator_dot_noalloc: %d x %d needs %zu rows of tiles of %d cells; a launch takes at most 65535",
+              w, h, tile_rows_y, tile_rows<double>());
+    return DT_UNSUPPORTED;
+  }
+  const size_t tiles = (size_t)ceil_div((size_t)w, TBX) * tile_rows_y;
   if (tiles > NOALLOC_MAX_TILES) {
     set_error("dt_flex_operator_dot_noalloc: %d x %d needs %zu tiles of %d x %d cells; the fixed scratch holds %zu",
               w, h, tiles, TBX, tile_rows<double>(), NOALLOC_MAX_TILES);

@@ -128,11 +128,13 @@ dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, con
  * allocate device memory at the point of use (a host code that gives the whole device to its own
  * fixed arena, or one that must not synchronise the device, as cudaMalloc and cudaFree can). The
  * reduction's scratch is a fixed device array inside this library: rasters up to
- * DT_NOALLOC_MAX_TILES tiles of 64 x 16 cells (134,217,728 cells, e.g. 16384 x 8192); larger
- * ones return DT_UNSUPPORTED. vav is a device pointer, written on `stream` (cudaStream_t as
+ * DT_NOALLOC_MAX_TILES tiles of 64 x 16 cells (134,217,728 cells, e.g. 16384 x 8192) and at most
+ * 65535 rows of tiles (h <= 1,048,560); larger ones return DT_UNSUPPORTED. vav is a device pointer, written on `stream` (cudaStream_t as
  * void*; NULL = the legacy default stream) in stream order; the call does not synchronise.
  * The first call on each device looks the scratch up (this can load the library's device code),
- * so make it before any stream capture that contains the call. The scratch is shared by every
+ * so make it before any stream capture that contains the call. The address found is kept for the
+ * life of the process: after a cudaDeviceReset by the caller it is stale, so a process that
+ * resets a device must not call this entry point on that device again. The scratch is shared by every
  * call on a device: calls that can overlap (other streams, other threads) race on it and must be
  * ordered by the caller. */
 #define DT_NOALLOC_MAX_TILES 131072

@@ -23,6 +23,8 @@
 #include <limits>
 #include <vector>
 
+#include <omp.h>
+
 #include "fft.hpp"
 #include "oracle.h"
 
@@ -668,6 +670,11 @@ void binomial(size_t w, size_t h, size_t passes, double* v) {
 using namespace oracle;
 
 extern "C" {
+
+// The OpenMP team size of the oracle's parallel loops (the timing legs run it at all host
+// threads and at 8, the reference's own benchmark setting); 0 or less restores all threads.
+void dto_set_threads(int n) { omp_set_num_threads(n > 0 ? n : omp_get_num_procs()); }
+int dto_threads(void) { return omp_get_max_threads(); }
 
 double dto_rigidity_per_g(double te_km, double g) { return rigidity_per_g(te_km, g); }
 double dto_flexural_parameter_m(double d_per_g) { return flexural_parameter_m(d_per_g); }

@@ -19,6 +19,8 @@ typedef struct {
   double rel_residual; /* ||r||_2 / ||b||_2 of the recurrence residual at exit */
 } dto_report;
 
+void dto_set_threads(int n);
+int dto_threads(void);
 double dto_rigidity_per_g(double te_km, double g);
 double dto_flexural_parameter_m(double d_per_g);
 int dto_flex_spectral_roundtrip(int w, int h, double dx, const double* v, double* out);

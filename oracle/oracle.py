@@ -73,6 +73,12 @@ def _f64(a):
 D = ctypes.c_double
 
 
+def set_threads(n: int) -> int:
+    """Run the oracle's OpenMP loops on n threads (n <= 0: all host threads); returns the count."""
+    lib().dto_set_threads(int(n))
+    return int(lib().dto_threads())
+
+
 def rigidity_per_g(te_km: float, g: float) -> float:
     return lib().dto_rigidity_per_g(te_km, g)
 

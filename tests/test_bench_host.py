@@ -50,3 +50,21 @@ def test_two_gloo_ranks_take_the_max_and_only_rank0_runs_the_reference_arm():
     assert sorted(r["rank"] for r in results) == [0, 1]
     assert all(r["world"] == 2 and r["max"] == 20.5 for r in results)
     assert all(r["reference_output"] == "" for r in results)
+
+
+def test_bench_launches_its_own_ranks_when_torchrun_did_not():
+    """`python bench.py --gpus 2` with no torchrun environment starts two gloo ranks itself; the
+    reference arm runs on rank 0 alone, whose line reports both ranks, and rank 1 prints nothing."""
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    p = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--impl", "reference",
+                        "--raster", "128,64,10000,4", "--steps", "2", "--warmup", "1", "--inputs", "1"],
+                       env=env, capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [json.loads(x) for x in p.stdout.splitlines() if x.startswith("{")]
+    assert len(lines) == 1, p.stdout
+    line = lines[0]
+    assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["steps"] == 2 and line["warmup"] == 1
+    assert "@128x64" in line["metric"] and line["value"] > 0
+    assert abs(line["ms_per_step"] * line["steps"] / 1e3 - 2 / line["value"]) < 1e-9

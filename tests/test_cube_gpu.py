@@ -79,3 +79,25 @@ def test_a_level_field_stays_level_on_the_device(case):
     got, rep = dev.solve(level, kd, 30.0, 1e-6)
     assert rep.iterations == 0
     assert np.allclose(got, level, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("n", [8, 32, 64])
+def test_the_one_block_coarse_cycle_is_bit_for_bit_the_separate_launches(n, monkeypatch):
+    """The coarse levels' cycle in one block (the default) against every level launching its own
+    kernels (DT_CUBE_FUSE_CELLS=0 at dt_cube_create): the same phases in the same order, so the
+    same bits. At n = 8 every level runs in the block; at 32 and 64 the finer levels launch."""
+    slots = O.cube_topology(n)
+    lap, areas, kd, h = cube_case(n, n + 200, slots)
+    r = np.random.default_rng(n).standard_normal(6 * n * n)
+    fused = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.setenv("DT_CUBE_FUSE_CELLS", "0")
+    apart = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.delenv("DT_CUBE_FUSE_CELLS")
+    for dt in (7.0, 60.0):
+        a, b = fused.vcycle(kd, dt, r), apart.vcycle(kd, dt, r)
+        assert np.array_equal(a, b), float(np.abs(a - b).max())
+        # twice in a row: the second cycle runs on the other buffer layout
+        assert np.array_equal(fused.vcycle(kd, dt, r), apart.vcycle(kd, dt, r))
+    xa, ra = fused.solve(h, kd, 7.0, 1e-6)
+    xb, rb = apart.solve(h, kd, 7.0, 1e-6)
+    assert ra.iterations == rb.iterations and np.array_equal(xa, xb)

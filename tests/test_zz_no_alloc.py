@@ -78,3 +78,6 @@ def test_a_zero_vector_does_not_stick_and_oversize_rasters_are_refused():
     # 16384 x 8208 needs 256 x 513 tiles, past the fixed scratch: refused before any device work
     assert call(lib, 16384, 8208, dx, td, tc, tv, ty, tvav, stream) == L.DT_UNSUPPORTED
     assert "fixed scratch" in L.last_error()
+    # 64 x 1,100,000 fits the scratch (68,750 tiles) but not a launch's 65535 rows of tiles
+    assert call(lib, 64, 1_100_000, dx, td, tc, tv, ty, tvav, stream) == L.DT_UNSUPPORTED
+    assert "rows of tiles" in L.last_error()
