@@ -31,6 +31,7 @@
 #include <algorithm>
 #include <utility>
 #include <cmath>
+#include <complex>
 #include <cstdarg>
 #include <cstdlib>
 #include <cstring>
@@ -1449,6 +1450,8 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   }
 }
 
+#include "rows_any.cuh"
+
 // ---------------------------------------------------------------------------------------------
 // Small control kernels.
 
@@ -1612,6 +1615,13 @@ struct Lane {
   T* row_factors = nullptr;
   T* row_transfer = nullptr;
   cplx<T>* row_state = nullptr;
+  // widths whose half is not a power of two (rows_any.cuh): per bank level two buffers of
+  // pairs x L complex values, the passes' twiddles (L), and for Bluestein the chirp (w) and the
+  // chirp's transform (L)
+  cplx<T>* any_buf = nullptr;
+  cplx<T>* any_tw = nullptr;
+  cplx<T>* any_chirp = nullptr;
+  cplx<T>* any_bhat = nullptr;
   Tables<T> tab;
   Scalars* S = nullptr;
   cudaGraph_t graph[4] = {};       // [(levels == 3) + 2 * reliable]
@@ -1624,7 +1634,9 @@ static const long double PI_L = 3.14159265358979323846264338327950288L;
 }  // namespace dt
 
 struct dt_flex {
-  int w = 0, h = 0, N = 0;
+  int w = 0, h = 0, N = 0;  // N = ceil(w / 2): complex values a row of the packed half spectrum
+  bool any = false;         // the transform along x by rows_any.cuh (w / 2 not a power of two)
+  dt::AnyPlan plan;
   double dx = 0;
   size_t n = 0;
   cudaStream_t stream = nullptr;
@@ -1716,6 +1728,104 @@ static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
   return DT_OK;
 }
 
+// The plan of the transform along x for a width whose half is not a power of two: mixed-radix
+// stages when every prime factor of w is at most ANY_MAX_PRIME, else Bluestein through the power
+// of two M >= 2 w - 1.
+static AnyPlan make_any_plan(int w, int h) {
+  AnyPlan p;
+  p.w = w;
+  p.pairs = (h + 1) / 2;
+  std::vector<int> f;
+  int n = w;
+  for (int r : {16, 8, 4, 2})
+    while (n % r == 0) {
+      f.push_back(r);
+      n /= r;
+    }
+  for (int q = 3; q <= ANY_MAX_PRIME && n > 1; q += 2)
+    while (n % q == 0) {
+      f.push_back(q);
+      n /= q;
+    }
+  if (n > 1) {  // a prime factor beyond ANY_MAX_PRIME
+    p.bluestein = 1;
+    int m = 1;
+    while (m < 2 * w - 1) m *= 2;
+    f.clear();
+    for (int r : {16, 8, 4, 2})
+      while (m % r == 0) {
+        f.push_back(r);
+        m /= r;
+      }
+  }
+  p.L = 1;
+  for (int x : f) p.L *= x;
+  p.nst = (int)f.size();
+  int span = 1;
+  for (int k = 0; k < p.nst; ++k) {
+    p.radix[k] = f[k];
+    p.span[k] = span;
+    span *= f[k];
+  }
+  return p;
+}
+
+// Host FFT in long double (iterative radix 2, length a power of two): Bluestein's table B.
+static void host_fft(std::vector<std::complex<long double>>& a) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    for (size_t i = 0; i < n; i += len)
+      for (size_t k = 0; k < len / 2; ++k) {
+        long double ang = -2.0L * PI_L * (long double)k / (long double)len;
+        std::complex<long double> t = a[i + k + len / 2] * std::complex<long double>(cosl(ang), sinl(ang));
+        a[i + k + len / 2] = a[i + k] - t;
+        a[i + k] += t;
+      }
+  }
+}
+
+template <class T>
+static dt_status make_any_tables(dt_flex* s, Lane<T>& L) {
+  using C = cplx<T>;
+  const AnyPlan& p = s->plan;
+  std::vector<C> tw(p.L);
+  for (int t = 0; t < p.L; ++t) {
+    long double ang = -2.0L * PI_L * t / p.L;
+    tw[t] = mk<C>((T)cosl(ang), (T)sinl(ang));
+  }
+  DT_TRY(dalloc(s, &L.any_tw, p.L));
+  DT_CUDA(cudaMemcpy(L.any_tw, tw.data(), p.L * sizeof(C), cudaMemcpyHostToDevice));
+  DT_TRY(dalloc(s, &L.any_buf, (size_t)3 * 2 * p.pairs * p.L));
+  if (p.bluestein) {
+    // c_n = e^(i pi n^2 / w) with n^2 reduced mod 2 w; b_n = c_n, b_(M - n) = c_n; B = FFT_M(b)
+    const int w = p.w;
+    std::vector<C> chirp(w);
+    std::vector<std::complex<long double>> b(p.L, 0.0L);
+    for (int q = 0; q < w; ++q) {
+      long long m = ((long long)q * q) % (2LL * w);
+      long double ang = PI_L * (long double)m / (long double)w;
+      std::complex<long double> c(cosl(ang), sinl(ang));
+      chirp[q] = mk<C>((T)c.real(), (T)c.imag());
+      b[q] = c;
+      if (q > 0) b[p.L - q] = c;
+    }
+    host_fft(b);
+    std::vector<C> bh(p.L);
+    for (int q = 0; q < p.L; ++q) bh[q] = mk<C>((T)b[q].real(), (T)b[q].imag());
+    DT_TRY(dalloc(s, &L.any_chirp, w));
+    DT_TRY(dalloc(s, &L.any_bhat, p.L));
+    DT_CUDA(cudaMemcpy(L.any_chirp, chirp.data(), w * sizeof(C), cudaMemcpyHostToDevice));
+    DT_CUDA(cudaMemcpy(L.any_bhat, bh.data(), p.L * sizeof(C), cudaMemcpyHostToDevice));
+  }
+  return DT_OK;
+}
+
 template <class T>
 static dt_status make_lane(dt_flex* s, Lane<T>& L) {
   size_t n = s->n;
@@ -1736,6 +1846,7 @@ static dt_status make_lane(dt_flex* s, Lane<T>& L) {
     }
   }
   DT_TRY(make_tables(s, L.tab));
+  if (s->any) DT_TRY(make_any_tables(s, L));
   DT_TRY(dalloc(s, &L.S, 1));
   DT_CUDA(cudaMemset(L.S, 0, sizeof(Scalars)));
   return DT_OK;
@@ -1973,9 +2084,103 @@ static void transform_smem_attributes() {
   }
 }
 
+// ---- the transform along x for any width (rows_any.cuh) ----
+static unsigned int any_grid(size_t threads) { return ceil_div(threads, 256); }
+
+// One FFT of length L over all row pairs: the stages alternate between a and b; returns the
+// buffer holding the result.
+template <class T>
+static cplx<T>* any_fft(dt_flex* s, Lane<T>& L, cplx<T>* a, cplx<T>* b, Scalars* S, cudaStream_t st) {
+  const AnyPlan& p = s->plan;
+  for (int k = 0; k < p.nst; ++k) {
+    const int R = p.radix[k];
+    const size_t bf = (size_t)p.pairs * (p.L / R);
+    switch (R) {
+      case 2: k_any_stage<T, 2><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 3: k_any_stage<T, 3><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 4: k_any_stage<T, 4><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 5: k_any_stage<T, 5><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 7: k_any_stage<T, 7><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 8: k_any_stage<T, 8><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      case 16: k_any_stage<T, 16><<<any_grid(bf), 256, 0, st>>>(p, k, a, b, L.any_tw, S); break;
+      default:
+        k_any_stage_prime<T><<<any_grid((size_t)p.pairs * p.L), 256, 0, st>>>(p, k, a, b, L.any_tw, S);
+        break;
+    }
+    counted();
+    std::swap(a, b);
+  }
+  return a;
+}
+
+// DFT_w of each row pair from buffer a (b is scratch); returns the buffer holding the DFT's
+// pass output (Bluestein: its second FFT, which any_fetch turns into the DFT).
+template <class T>
+static cplx<T>* any_dft(dt_flex* s, Lane<T>& L, cplx<T>* a, cplx<T>* b, Scalars* S, cudaStream_t st) {
+  cplx<T>* f = any_fft<T>(s, L, a, b, S, st);
+  if (s->plan.bluestein) {
+    k_any_chirp_mul<T><<<any_grid((size_t)s->plan.pairs * s->plan.L), 256, 0, st>>>(s->plan, f, L.any_bhat, S);
+    counted();
+    f = any_fft<T>(s, L, f, f == a ? b : a, S, st);
+  }
+  return f;
+}
+
+// The level's scratch pair: 2 x pairs x L complex values a level.
+template <class T>
+static cplx<T>* any_slot(dt_flex* s, Lane<T>& L, int level) {
+  return L.any_buf + (size_t)level * 2 * s->plan.pairs * s->plan.L;
+}
+
+template <class T>
+static void any_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cplx<T>* half, int level, Scalars* S,
+                         cudaStream_t st) {
+  const AnyPlan& p = s->plan;
+  cplx<T>* a = any_slot<T>(s, L, level);
+  cplx<T>* b = a + (size_t)p.pairs * p.L;
+  const unsigned g = any_grid((size_t)p.pairs * p.L);
+  if (wt)
+    k_any_load_rows<T, true><<<g, 256, 0, st>>>(p, s->h, in, wt, a, L.any_chirp, S);
+  else
+    k_any_load_rows<T, false><<<g, 256, 0, st>>>(p, s->h, in, wt, a, L.any_chirp, S);
+  counted();
+  cplx<T>* f = any_dft<T>(s, L, a, b, S, st);
+  k_any_split<T><<<any_grid((size_t)p.pairs * s->N), 256, 0, st>>>(p, s->h, s->N, f, half, L.any_chirp, S);
+  counted();
+}
+
+template <class T>
+static void any_rows_inv(dt_flex* s, Lane<T>& L, int mode, const cplx<T>* half, T* out, const T* wt, const T* r,
+                         Scalars* S, cudaStream_t st) {
+  const AnyPlan& p = s->plan;
+  const int levels = mode == INV_BANK ? 3 : 1;
+  const size_t pl = (size_t)p.pairs * p.L;
+  cplx<T>* f0 = nullptr;
+  for (int lv = 0; lv < levels; ++lv) {
+    cplx<T>* a = any_slot<T>(s, L, lv);
+    k_any_load_half<T><<<any_grid(pl), 256, 0, st>>>(p, s->h, s->N, half + (size_t)lv * s->h * s->N, a, L.any_chirp, S);
+    counted();
+    cplx<T>* f = any_dft<T>(s, L, a, a + pl, S, st);
+    if (lv == 0) f0 = f;  // every level ends in the same buffer of its pair
+  }
+  const unsigned g = std::min<unsigned>(any_grid((size_t)p.pairs * p.w), (unsigned)s->sms * 4);
+  const size_t stride = 2 * pl;
+  switch (mode) {
+    case INV_STORE: k_any_emit<T, INV_STORE><<<g, 256, 0, st>>>(p, s->h, f0, stride, out, wt, r, L.any_chirp, s->partials, S); break;
+    case INV_STORE_W: k_any_emit<T, INV_STORE_W><<<g, 256, 0, st>>>(p, s->h, f0, stride, out, wt, r, L.any_chirp, s->partials, S); break;
+    case INV_BANK: k_any_emit<T, INV_BANK><<<g, 256, 0, st>>>(p, s->h, f0, stride, out, wt, r, L.any_chirp, s->partials, S); break;
+    default: k_any_emit<T, INV_STORE_DOT><<<g, 256, 0, st>>>(p, s->h, f0, stride, out, wt, r, L.any_chirp, s->partials, S); break;
+  }
+  counted();
+}
+
 template <class T>
 static void launch_rows_fwd(dt_flex* s, Lane<T>& L, const T* in, const T* wt, cplx<T>* half, const FftGeo& g, Scalars* S,
-                            cudaStream_t st) {
+                            cudaStream_t st, int level = 0) {
+  if (s->any) {
+    any_rows_fwd<T>(s, L, in, wt, half, level, S, st);
+    return;
+  }
   int logn = ilog2(s->N);
   if (wt)
     rows_fwd_fn<T, true>(logn, LogSeq{})<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, in, wt, half, L.tab.tw_row,
@@ -2020,6 +2225,10 @@ static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, 
 template <class T>
 static void launch_rows_inv(dt_flex* s, Lane<T>& L, int mode, const cplx<T>* half, T* out, const T* wt, const T* r,
                             const FftGeo& g, Scalars* S, cudaStream_t st) {
+  if (s->any) {
+    any_rows_inv<T>(s, L, mode, half, out, wt, r, S, st);
+    return;
+  }
   rows_inv_for<T>(mode, ilog2(s->N))<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, half, out, wt, r, L.tab.tw_row,
                                                                            L.tab.post, s->partials, S);
   counted();
@@ -2056,7 +2265,7 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
   cudaStream_t lst[3] = {st, s->side[0], s->side[1]};
   cplx<T>* lh[3] = {L.half, L.half_side[0], L.half_side[1]};
   for (int k = 0; k < 3; ++k) {
-    launch_rows_fwd<T>(s, L, L.left, L.wt[k], lh[k], g, L.S, lst[k]);
+    launch_rows_fwd<T>(s, L, L.left, L.wt[k], lh[k], g, L.S, lst[k], k);
     launch_cols<T>(s, L, lh[k], g, k, L.S, lst[k]);
   }
   cudaEventRecord(s->ev_join[0], s->side[0]);
@@ -2633,12 +2842,12 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     set_error("dt_flex_create: bad raster %d x %d, dx %g", w, h, dx);
     return DT_BAD_ARG;
   }
-  // the transform along x needs w/2 a power of two; along y the cosine transform needs h one,
-  // and any other h is solved per wavenumber (the row solve, with the block metric's couplings
-  // when no metric is given)
-  if ((w & 1) || !is_pow2(w / 2) || w / 2 > 8192 || h > 8192) {
-    set_error("dt_flex_create: the device transforms need w/2 a power of two, at most 8192, and h at most 8192 "
-              "(got %d x %d)", w, h);
+  // the transform along x takes any width: the shared-memory kernels when w/2 is a power of two
+  // up to 8192, the passes of rows_any.cuh otherwise; along y the cosine transform takes a
+  // power-of-two h, and any other h is solved per wavenumber (the row solve, with the block
+  // metric's couplings when no metric is given)
+  if (w > 65536 || h > 8192) {
+    set_error("dt_flex_create: the device transforms take w up to 65536 and h up to 8192 (got %d x %d)", w, h);
     return DT_UNSUPPORTED;
   }
   if (!metric_a != !metric_b) {
@@ -2665,7 +2874,9 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   auto* s = new dt_flex();
   s->w = w;
   s->h = h;
-  s->N = w / 2;
+  s->any = (w & 1) || !is_pow2(w / 2) || w / 2 > 8192;
+  s->N = (w + 1) / 2;
+  if (s->any) s->plan = make_any_plan(w, h);
   s->dx = dx;
   s->n = (size_t)w * h;
   cudaDeviceProp prop;

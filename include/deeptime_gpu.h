@@ -102,10 +102,13 @@ void dt_flex_default_params(dt_flex_params* p);
  * one without the other is DT_BAD_ARG. On the row metric the operator runs the per-block stencil
  * with the rows' couplings, the Jacobi weights take (L D L)'s diagonal on the metric, and the
  * spectral pass solves d L_k^2 + c per wavenumber along y (RowSolve, :1012-1099) in place of the
- * cosine transform, so h need not be a power of two (w/2 still must). On the block metric a
- * height that is not a power of two takes the same row solve with the block couplings
- * (RowMetric::block: a = 1, b = 1 inside and 0 at the edges), the cosine transform's inverse;
- * the operator and the Jacobi weights stay the block metric's. */
+ * cosine transform, so h need not be a power of two. On the block metric a height that is not a
+ * power of two takes the same row solve with the block couplings (RowMetric::block: a = 1, b = 1
+ * inside and 0 at the edges), the cosine transform's inverse; the operator and the Jacobi weights
+ * stay the block metric's. Any width from 2 to 65536 is taken, as the reference plans its FFT at
+ * any length (Spectral::new, flexure.rs:1139-1170): w/2 a power of two up to 8192 through one
+ * shared-memory kernel a pass, every other width through mixed-radix passes (prime factors up to
+ * 64) or Bluestein's chirp z-transform. h is at most 8192; larger rasters are DT_UNSUPPORTED. */
 dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const double* metric_b, dt_flex** out);
 dt_status dt_flex_destroy(dt_flex* s);
 /* Binds the handle to a CUDA stream (cudaStream_t passed as void*); NULL = the handle's own. */
