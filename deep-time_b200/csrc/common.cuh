@@ -3,6 +3,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -193,6 +195,15 @@ void begin_capture_count();
 long long end_capture_count();
 
 inline unsigned int ceil_div(size_t a, size_t b) { return (unsigned int)((a + b - 1) / b); }
+
+// Test support for the allocation failure path: with DT_FAIL_ALLOC_AT=n in the environment, the
+// n-th device allocation of a handle (its counter `made`, from 1) fails as if the device were out
+// of memory. Without the variable every allocation goes to cudaMalloc.
+inline bool alloc_fault(size_t& made) {
+  ++made;
+  const char* e = getenv("DT_FAIL_ALLOC_AT");
+  return e && e[0] && (size_t)strtoull(e, nullptr, 10) == made;
+}
 inline bool is_pow2(long v) { return v > 0 && (v & (v - 1)) == 0; }
 inline int ilog2(long v) {
   int r = 0;

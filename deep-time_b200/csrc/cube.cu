@@ -567,6 +567,7 @@ struct dt_cube {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   std::vector<void*> allocs;
+  size_t nalloc = 0;  // device allocations made (the DT_FAIL_ALLOC_AT test hook counts them)
   uint32_t* slots = nullptr;
   double *lap = nullptr, *mu = nullptr;
   double *kd = nullptr, *h = nullptr;  // staging for the host entry points
@@ -594,6 +595,10 @@ namespace {
 template <class T>
 dt_status cube_alloc(dt_cube* s, T** p, size_t count) {
   void* q = nullptr;
+  if (alloc_fault(s->nalloc)) {
+    set_error("cudaMalloc of %zu bytes failed: out of memory (DT_FAIL_ALLOC_AT)", count * sizeof(T));
+    return DT_OOM;
+  }
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) {
     set_error("dt_cube: cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));

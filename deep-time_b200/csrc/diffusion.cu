@@ -791,6 +791,7 @@ struct dt_diff {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
   std::vector<void*> allocs;
+  size_t nalloc = 0;  // device allocations made (the DT_FAIL_ALLOC_AT test hook counts them)
   double *kd = nullptr, *b = nullptr, *x = nullptr, *r = nullptr, *p = nullptr, *ap = nullptr;
   double *east = nullptr, *south = nullptr, *diag = nullptr;
   float *east32 = nullptr, *south32 = nullptr, *diag32 = nullptr;
@@ -809,6 +810,10 @@ namespace dt {
 template <class T>
 static dt_status ddalloc(dt_diff* s, T** p, size_t count) {
   void* q = nullptr;
+  if (alloc_fault(s->nalloc)) {
+    set_error("cudaMalloc of %zu bytes failed: out of memory (DT_FAIL_ALLOC_AT)", count * sizeof(T));
+    return DT_OOM;
+  }
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) {
     set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));

@@ -83,6 +83,7 @@ struct Scalars {
   int replacements;         // residual replacements so far
   unsigned long long cond_if;  // the loop body's IF node around the replacement, 0 without one
   int fault;                // a kernel's bounded wait ran out (the solve reports a device error)
+  int wait_give_up;         // test support: the TMA stencil's tile waits give up at once
 };
 
 __device__ __forceinline__ void set_cond(Scalars* S, unsigned int v) {
@@ -1512,7 +1513,9 @@ __global__ void k_begin(Scalars* S) {
   S->started = 0;
   S->body_runs = 0;
   S->err = 0.0;
-  if (!isfinite(S->bb) || !isfinite(S->rr)) {
+  if (S->fault) {
+    S->stop = STOP_NONFINITE;  // a wait ran out before the loop: it does not start
+  } else if (!isfinite(S->bb) || !isfinite(S->rr)) {
     S->stop = STOP_NONFINITE;
   } else if (!(S->bb > 0.0)) {
     S->stop = STOP_CONVERGED;  // b = 0: x = 0 is exact
@@ -1655,6 +1658,10 @@ struct dt_flex {
   double* unet_sums = nullptr;     // sum of b_coarse^2 and of c
   double* rzpair = nullptr;        // warm start: b.M^-1 b and r0.M^-1 r0
   std::vector<void*> allocs;
+  size_t nalloc = 0;  // device allocations made (the DT_FAIL_ALLOC_AT test hook counts them)
+  // test support: DT_STENCIL_WAIT_GIVE_UP=1 at create makes the TMA stencil's tile waits give up
+  // without testing their barrier, so the solve takes the path of a wait that ran out
+  int wait_give_up = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
@@ -1683,6 +1690,10 @@ namespace dt {
 template <class T>
 static dt_status dalloc(dt_flex* s, T** p, size_t count) {
   void* q = nullptr;
+  if (alloc_fault(s->nalloc)) {
+    set_error("cudaMalloc of %zu bytes failed: out of memory (DT_FAIL_ALLOC_AT)", count * sizeof(T));
+    return DT_OOM;
+  }
   cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
   if (e != cudaSuccess) {
     set_error("cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
@@ -2443,9 +2454,11 @@ struct HostProblem {
   int max_it;
   int rule;
   int n;
+  int wait_give_up;
 };
 __global__ void k_put_problem(Scalars* S, HostProblem p) {
   S->fault = 0;
+  S->wait_give_up = p.wait_give_up;
   S->tol = p.tol;
   S->max_it = p.max_it;
   S->rule = p.rule;
@@ -2618,7 +2631,7 @@ static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_r
   cudaStream_t st = s->stream;
   int levels = 1;
   DT_TRY(setup_precond<double>(s, L, p->precond, &levels));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n, s->wait_give_up}); counted();
   norm_b<double>(s, s->b64, L.S);
   DT_TRY(warm_or_cold(s, warm, L, levels));
   DT_TRY(run_pcg<double>(s, L, levels, p->host_loop));
@@ -2635,6 +2648,10 @@ static dt_status solve_fp64(dt_flex* s, const dt_flex_params* p, bool warm, dt_r
   // the true residual of the answer
   resid64(s);
   DT_TRY(read_scalars(s, L.S, &h));
+  if (h.fault) {
+    set_error("flexure solve: a kernel's wait for its tile copies ran out");
+    return DT_DEVICE_ERROR;
+  }
   h.err = err;
   DT_TRY(fill_report(s, h, iterations, 0, rep));
   if (rep) {
@@ -2664,7 +2681,7 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
   k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
   int levels = 1;
   DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n, s->wait_give_up}); counted();
   norm_b<double>(s, s->b64, L.S);
   DT_TRY(warm_or_cold(s, warm, F, levels));
   int iterations = 0, refinements = 0;
@@ -2674,6 +2691,10 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
   bool converged = false, nonfinite = false;
   for (;;) {
     DT_TRY(read_scalars(s, L.S, &h));
+    if (h.fault) {
+      set_error("flexure solve: a kernel's wait for its tile copies ran out");
+      return DT_DEVICE_ERROR;
+    }
     if (!std::isfinite(h.rr) || !std::isfinite(h.bb)) {
       nonfinite = true;
       break;
@@ -2687,7 +2708,7 @@ static dt_status solve_mixed(dt_flex* s, const dt_flex_params* p, bool warm, dt_
     if (refinements >= p->max_refinements || iterations >= p->max_iterations) break;
     double itol = std::min(0.5, std::max(p->inner_tol, 0.3 * lim / rel));
     k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale); counted();
-    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{itol, p->max_iterations - iterations, DT_STOP_REL_RESIDUAL, (int)s->n, s->wait_give_up}); counted();
     norm_b<float>(s, F.r, F.S);
     k_rr_is_bb<<<1, 1, 0, st>>>(F.S); counted();  // x = 0: r = b
     DT_TRY(run_pcg<float>(s, F, levels, p->host_loop));
@@ -2740,11 +2761,11 @@ static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool 
   k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
   int levels = 1;
   DT_TRY(setup_precond<float>(s, F, p->precond, &levels));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n}); counted();
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{p->tol, p->max_iterations, p->stop, (int)s->n, s->wait_give_up}); counted();
   norm_b<double>(s, s->b64, L.S);
   DT_TRY(warm_or_cold(s, warm, F, levels));
   k_scale_down<<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r, F.x, L.S, s->scale); counted();
-  k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{p->tol, p->max_iterations, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
+  k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{p->tol, p->max_iterations, DT_STOP_REL_RESIDUAL, (int)s->n, s->wait_give_up}); counted();
   k_reliable_init<<<1, 1, 0, st>>>(F.S, L.S, s->scale, p->tol, p->max_iterations, RELIABLE_DELTA,
                                    p->stop == DT_STOP_RMS_RESIDUAL ? 1 : 0);
   counted();
@@ -2755,13 +2776,13 @@ static dt_status solve_mixed_reliable(dt_flex* s, const dt_flex_params* p, bool 
   resid64(s);
   Scalars h, hf;
   DT_TRY(read_scalars(s, F.S, &hf));
-  if (hf.fault) {
+  DT_TRY(read_scalars(s, L.S, &h));
+  if (hf.fault || h.fault) {  // either lane's stencil (the FP64 residual's too)
     set_error("flexure solve: a kernel's wait for its tile copies ran out");
     return DT_DEVICE_ERROR;
   }
   count_loop(F, levels, p->host_loop, hf.body_runs, true);
   if (!p->host_loop) g_launches += 3LL * hf.replacements;  // the IF node's kernels, when they ran
-  DT_TRY(read_scalars(s, L.S, &h));
   bool nonfinite = hf.stop == STOP_NONFINITE || !std::isfinite(h.rr) || !std::isfinite(h.bb);
   double bref = p->stop == DT_STOP_RMS_RESIDUAL ? (double)s->n : h.bb;
   bool converged = !nonfinite && (h.bb <= 0 || h.rr <= p->tol * p->tol * bref);
@@ -2891,6 +2912,7 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
     return fail(DT_DEVICE_ERROR);
   }
   s->own_stream = true;
+  if (const char* e = getenv("DT_STENCIL_WAIT_GIVE_UP")) s->wait_give_up = e[0] == '1';
   // RowMetric::block (flexure.rs:1000-1010): the block metric's couplings, for a height the
   // cosine transform does not take
   std::vector<double> block_a, block_b;
@@ -3232,13 +3254,13 @@ dt_status dt_flex_precondition(dt_flex* s, const double* d, const double* c, con
   DT_CUDA(cudaMemcpyAsync(L.d, d, bytes, cudaMemcpyHostToDevice, st));
   DT_CUDA(cudaMemcpyAsync(L.c, c, bytes, cudaMemcpyHostToDevice, st));
   DT_CUDA(cudaMemcpyAsync(L.r, r, bytes, cudaMemcpyHostToDevice, st));
-  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
+  k_put_problem<<<1, 1, 0, st>>>(L.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n, s->wait_give_up}); counted();
   if (precision == DT_PREC_MIXED) {
     Lane<float>& F = s->L32;
     k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.d, F.d); counted();
     k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.c, F.c); counted();
     k_convert<double, float><<<ew_grid(s), 256, 0, st>>>(s->n, L.r, F.r); counted();
-    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n}); counted();
+    k_put_problem<<<1, 1, 0, st>>>(F.S, HostProblem{0.0, 0, DT_STOP_REL_RESIDUAL, (int)s->n, s->wait_give_up}); counted();
     int levels;
     DT_TRY(setup_precond<float>(s, F, precond, &levels));
     k_reset<<<1, 1, 0, st>>>(F.S); counted();

@@ -41,10 +41,10 @@ __device__ __forceinline__ bool mbar_test_wait(uint32_t a, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait for the phase with parity `parity` to complete: 2^24 tests with a short sleep
-// between them (well under a second in all), false when it did not complete.
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity) {
-  for (int it = 0; it < (1 << 24); ++it) {
+// Bounded wait for the phase with parity `parity` to complete: `polls` tests (2^24 by default)
+// with a short sleep between them (well under a second in all), false when it did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t a, uint32_t parity, int polls = 1 << 24) {
+  for (int it = 0; it < polls; ++it) {
     if (mbar_test_wait(a, parity)) return true;
     if (it > 64) __nanosleep(20);
   }
@@ -149,7 +149,8 @@ __global__ void __launch_bounds__(TBX* TTY) k_apply_tma(const __grid_constant__ 
   for (int t = blockIdx.x; t < ntiles; t += G, ++k) {
     const int b = k & 1;
     if (tid == 0) {
-      if (!mbar_wait_bounded(smem_u32(&mbar[b]), phase[b])) s_fail = 1;
+      // S->wait_give_up (a test of this path): no test at all, as if the wait had run out
+      if (!mbar_wait_bounded(smem_u32(&mbar[b]), phase[b], S->wait_give_up ? 0 : 1 << 24)) s_fail = 1;
       pending[b] = false;
     }
     phase[b] ^= 1u;
