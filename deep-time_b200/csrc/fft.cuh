@@ -227,6 +227,60 @@ struct Stages {
   }
 };
 
+// The adjoint of stockham_stage<C, R, EPT, false, LOGN, NS> (inverse twiddles and DFT, the read
+// and write patterns swapped): reads the positions that stage wrote, (j - k) R + k + r NS, takes
+// the inverse DFT, multiplies by the conjugated twiddles and writes the positions that stage read,
+// j + r N / R. Running a forward transform's stages' adjoints in reverse order gives N times its
+// inverse.
+template <class C, int R, int EPT, int LOGN, int NS, int PITCH = 0, int NTH = 0>
+__device__ __forceinline__ void stockham_stage_adj(C* s, const C* __restrict__ tw) {
+  constexpr int N = 1 << LOGN;
+  constexpr int NP = PITCH ? PITCH : Pad<C>::len(N);
+  constexpr int B = EPT / R;
+  constexpr int NBF = N / R;
+  constexpr int LOGNBF = LOGN - (R == 16 ? 4 : R == 8 ? 3 : R == 4 ? 2 : 1);
+  constexpr int STEP = N / (NS * R);
+  static_assert(NS % 16 == 0 && NBF % 16 == 0, "adjoint stage: spans of whole 16-slot groups");
+  const int tid = threadIdx.x;
+  C v[B][R];
+  int wbase[B], kk[B];
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    int t = tid + q * (NTH ? NTH : (int)blockDim.x);
+    int b = t >> LOGNBF;
+    int j = t & (NBF - 1);
+    int k = j & (NS - 1);
+    const C* src = s + b * NP + Pad<C>::at((j - k) * R + k);
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[q][r] = src[r * (NS + NS / 16)];
+    wbase[q] = b * NP + Pad<C>::at(j);
+    kk[q] = k;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < B; ++q) {
+    dft_r<C, R, true>(v[q]);
+    C w[R];
+    stage_twiddles<C, R, true>(tw, STEP * kk[q], w);
+    C* dst = s + wbase[q];
+    dst[0] = v[q][0];
+#pragma unroll
+    for (int r = 1; r < R; ++r) dst[r * (NBF + NBF / 16)] = cmul(v[q][r], w[r]);
+  }
+  __syncthreads();
+}
+
+// The adjoints of Stages<C, EPT, false, LOGN, NS, REM> in reverse order (the last stage's first).
+template <class C, int EPT, int LOGN, int NS, int REM, int PITCH = 0, int NTH = 0>
+struct StagesAdj {
+  static __device__ __forceinline__ void run(C* s, const C* __restrict__ tw) {
+    if constexpr (REM >= 4 && EPT % 16 == 0) {
+      StagesAdj<C, EPT, LOGN, NS * 16, REM - 4, PITCH, NTH>::run(s, tw);
+      stockham_stage_adj<C, 16, EPT, LOGN, NS, PITCH, NTH>(s, tw);
+    }
+  }
+};
+
 // The radix the stages above give a length-2^LOGN transform's last stage.
 __host__ __device__ constexpr int last_radix(int logn) {
   return logn % 4 == 0 ? 16 : (1 << (logn % 4));

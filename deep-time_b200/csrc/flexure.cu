@@ -710,6 +710,17 @@ enum { INV_STORE = 0, INV_STORE_DOT = 2, INV_STORE_W = 3, INV_BANK = 4 };
 // Correctly rounded reciprocals (double: one division; float: the intrinsic).
 __device__ __forceinline__ double recip(double x) { return 1.0 / x; }
 __device__ __forceinline__ float recip(float x) { return __frcp_rn(x); }
+// Reciprocals with no slow-path call, for code that keeps many values in registers around them:
+// float, the hardware's approximate reciprocal (__fdividef, at most 2 ulp for |x| in
+// [2^-126, 2^126]); double, that estimate refined by two Newton-Raphson steps r <- r + r (1 - x r)
+// (each squares the relative error: 2^-22 -> 2^-44 -> 2^-88). Used for the spectral divisors
+// d lambda^2 + c_ref, which lie in (c_ref, 1e36) for any raster this solver takes.
+__device__ __forceinline__ float recip_fast(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ double recip_fast(double x) {
+  double r = (double)__fdividef(1.0f, (float)x);
+  r = fma(r, fma(-x, r, 1.0), r);
+  return fma(r, fma(-x, r, 1.0), r);
+}
 constexpr int FFT_EPT = 16;
 constexpr int FFT_BATCH = 8;  // global loads a thread of a transform kernel keeps in flight
 constexpr int FFT_MAX_THREADS = 512;
@@ -832,7 +843,7 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
 // lx[k] = 2 cos(2 pi k / w) - 2 for k = 0..N; ly[m] = 2 cos(pi m / h) - 2.
 template <class T, int LOGH>
 __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_cols(int N, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
-                                                         const cplx<T>* __restrict__ omega, const T* __restrict__ lx,
+                                                         const cplx<T>* __restrict__ omega, const cplx<T>* __restrict__ omega2, const T* __restrict__ lx,
                                                          const T* __restrict__ ly, T inv_dx2, const Scalars* S, int level) {
   using C = cplx<T>;
   using P = Pad<C>;
@@ -990,6 +1001,211 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
           const int p = j + r * NSL, row = r < RL / 2 ? 2 * p : 2 * (h - 1 - p) + 1;
           half[(size_t)row * N + k] = cscale(v[r], inv_h);
         }
+      }
+    }
+  }
+}
+
+// The column pass with the divide in registers, for column lengths h = 2^LOGH whose last radix
+// RL = last_radix(LOGH) is below 16 (h = 32 .. 2048 except 256), so that a thread holds
+// B = FFT_EPT / RL >= 2 butterflies of the forward transform's last stage. The same values as
+// k_cols (forward DCT-II by Makhoul's reordering and one complex FFT, divide by d lambda^2 + c,
+// inverse DCT), with fewer shared-memory passes:
+//   - forward stages as k_cols (the first straight from global memory);
+//   - the last forward stage, span NS = h / RL, into registers: butterfly j's outputs are
+//     m = j + r NS, and the partner h - m of each is an output of butterfly NS - j (j = 0 and
+//     NS / 2 pair within themselves). A thread takes butterflies t + q T and their partners
+//     (T = NS / B threads a column), so every pair (m, h - m) the divide couples is its own;
+//   - the divide on the pair: with a = 1 / D_m, b = 1 / D_(h-m) (D = d lambda^2 + c_ref) and
+//     w2 = e^(-i pi m / h), V'_m = (a + b)/2 V_m + (a - b)/2 conj(w2) V_(h-m) and
+//     V'_(h-m) = (a - b)/2 w2 V_m + (a + b)/2 V_(h-m): the DCT twiddle, the divide and the inverse
+//     DCT twiddle of k_cols folded into one 2 x 2 map (column 0, packed with two real
+//     wavenumbers, keeps k_cols's separate form);
+//   - the inverse transform as the forward stages' adjoints in reverse order, the last stage's
+//     adjoint still in registers, the first stage's adjoint writing to global memory.
+// Shared memory is written four times a transform pair instead of six, with six block barriers
+// instead of nine.
+// e^(-i pi e / 8), e = 0 .. 7: the rotations between the DCT twiddles of one last-stage butterfly.
+template <class C>
+__device__ __forceinline__ C rot_pi(int e) {
+  using T = decltype(C::x);
+  const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173, h = (T)0.70710678118654752440;
+  switch (e & 7) {
+    case 0: return mk<C>((T)1, (T)0);
+    case 1: return mk<C>(c1, -s1);
+    case 2: return mk<C>(h, -h);
+    case 3: return mk<C>(s1, -c1);
+    case 4: return mk<C>((T)0, (T)-1);
+    case 5: return mk<C>(-s1, -c1);
+    case 6: return mk<C>(-h, -h);
+    default: return mk<C>(-c1, -s1);
+  }
+}
+
+// Columns a block of the fused pass: half of k_cols's, so that three blocks share an SM with
+// up to 85 registers a thread (the pass keeps two butterflies and their twiddles in registers).
+__host__ __device__ constexpr int cols_per_block_fused(int logh, int elem) {
+  return cols_per_block(logh, elem) > 1 ? cols_per_block(logh, elem) / 2 : 1;
+}
+
+template <class T, int LOGH>
+__global__ void __launch_bounds__(FFT_MAX_THREADS / 2, 3) k_cols_fused(int N, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
+                                                               const cplx<T>* __restrict__ omega, const cplx<T>* __restrict__ omega2,
+                                                               const T* __restrict__ lx, const T* __restrict__ ly, T inv_dx2,
+                                                               const Scalars* S, int level) {
+  using C = cplx<T>;
+  using P = Pad<C>;
+  if (S->stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  constexpr int h = 1 << LOGH;
+  constexpr int HP = col_pitch(h);
+  constexpr int CPB = cols_per_block_fused(LOGH, (int)sizeof(C));
+  constexpr int logc = CPB == 1 ? 0 : CPB == 2 ? 1 : CPB == 4 ? 2 : CPB == 8 ? 3 : CPB == 16 ? 4 : 5;
+  constexpr int NT = CPB * h / FFT_EPT;
+  constexpr int RL = last_radix(LOGH);
+  constexpr int LOGRL = RL == 8 ? 3 : RL == 4 ? 2 : 1;
+  constexpr int NS = h / RL;          // the last stage's span, and its butterflies a column
+  constexpr int B = FFT_EPT / RL;     // last-stage butterflies a thread
+  constexpr int TPC = h / FFT_EPT;    // threads a column
+  static_assert(RL < 16 && LOGH >= 5 && B >= 2 && NS % 16 == 0, "the fused column pass: a last radix below 16");
+  static_assert(TPC * CPB == NT, "columns: whole threads");
+  const int k0 = blockIdx.x * CPB;
+  const int tid = threadIdx.x;
+  const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
+  // ---- forward, first stage (radix 16, span 1) straight from global memory in Makhoul's order:
+  // thread tid takes butterfly j = tid / CPB of column tid % CPB, v[j + r h / 16]
+  {
+    const int cc = tid & (CPB - 1), j = tid >> logc, k = k0 + cc;
+    C v[16];
+    const int kk = k < N ? k : 0;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int p = j + r * (h / 16), row = r < 8 ? 2 * p : 2 * (h - 1 - p) + 1;
+      v[r] = half[row * N + kk];  // h N < 2^31: 32-bit offsets
+    }
+    if (k >= N) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) v[r] = mk<C>((T)0, (T)0);
+    }
+    dft_r<C, 16, false>(v);
+    C* col = s + cc * HP;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) col[17 * j + r] = v[r];  // pad(16 j + r) = 17 j + r
+    __syncthreads();
+  }
+  // ---- forward, middle stages (radix 16), spans 16 .. NS / 16
+  Stages<C, FFT_EPT, false, LOGH, 16, LOGH - 4 - LOGRL, HP, NT>::run(s, tw);
+  // ---- forward last stage, divide, its adjoint: in registers
+  {
+    const int cc = tid / TPC, t = tid & (TPC - 1), k = k0 + cc;
+    C* col = s + cc * HP;
+    constexpr int T2 = NS / B;  // = TPC: the thread's butterflies t + q T2 and their partners
+    int jb[B];
+#pragma unroll
+    for (int q = 0; q < B / 2; ++q) {
+      jb[q] = t + q * T2;
+      jb[q + B / 2] = (t == 0 && q == 0) ? NS / 2 : NS - jb[q];
+    }
+    C v[B][RL];
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      const C* src = col + P::at(jb[q]);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[q][r] = src[r * (NS + NS / 16)];
+      C w[RL];
+      stage_twiddles<C, RL, false>(tw, jb[q], w);  // the last stage's twiddles w_h^(r j)
+#pragma unroll
+      for (int r = 1; r < RL; ++r) v[q][r] = cmul(v[q][r], w[r]);
+      dft_r<C, RL, false>(v[q]);
+    }
+    if (k < N) {
+      const T lxk = lx[k];
+      auto rden = [&](T lxv, T lyv) {
+        T l = (lxv + lyv) * inv_dx2;
+        return recip_fast(dref * (l * l) + cref);
+      };
+      // the pair (m, h - m) held in (vm, vn); w2 = e^(-i pi m / h), and ly[m] = 2 cos(pi m / h) - 2
+      // = 2 Re(w2) - 2 (flexure.rs:1146), ly[h - m] = -ly[m] - 4
+      auto pair = [&](C& vm, C& vn, C w2, int m) {
+        const T ym = (T)2 * w2.x - (T)2, yn = -ym - (T)4;
+        if (k == 0) {  // packed: real part wavenumber 0, imaginary part N (k_cols's form)
+          const T lxn = lx[N];
+          const C wm = omega[m], wn = mk<C>(-wm.y, -wm.x);
+          C p = cmul(wm, vm), q = cmul(wn, vn);
+          C cm = cscale(cadd(p, cmuli(q)), (T)0.5), cn = cscale(cadd(q, cmuli(p)), (T)0.5);
+          cm.x *= rden(lxk, ym);
+          cm.y *= rden(lxn, ym);
+          cn.x *= rden(lxk, yn);
+          cn.y *= rden(lxn, yn);
+          vm = cmul(cconj(wm), csub(cm, cmuli(cn)));
+          vn = cmul(cconj(wn), csub(cn, cmuli(cm)));
+          return;
+        }
+        const T a = rden(lxk, ym), b = rden(lxk, yn);
+        const T sv = (a + b) * (T)0.5, tv = (a - b) * (T)0.5;
+        const C xm = vm, xn = vn;
+        vm = cadd(cscale(xm, sv), cscale(cmul(cconj(w2), xn), tv));
+        vn = cadd(cscale(cmul(w2, xm), tv), cscale(xn, sv));
+      };
+      // e^(-i pi m / h) for m = j + r NS: e^(-i pi j / h) e^(-i pi r / RL), one table load a butterfly
+      auto w2_at = [&](C w2j, int r) { return r == 0 ? w2j : cmul(w2j, rot_pi<C>(r * (8 / RL))); };
+#pragma unroll
+      for (int q = 0; q < B / 2; ++q) {
+        if (t == 0 && q == 0) {
+          // butterfly 0: m = r NS pairs with (RL - r) NS, m = 0 and h / 2 with themselves (for
+          // m = h / 2 both divisors are equal, so the pair form with vn = vm is the plain one)
+          if (k == 0) {
+            v[0][0].x *= rden(lxk, (T)0);
+            v[0][0].y *= rden(lx[N], (T)0);
+          } else {
+            v[0][0] = cscale(v[0][0], rden(lxk, (T)0));
+          }
+          const C one = mk<C>((T)1, (T)0);
+#pragma unroll
+          for (int r = 1; r < RL / 2; ++r) pair(v[0][r], v[0][RL - r], w2_at(one, r), r * NS);
+          {
+            C self = v[0][RL / 2];
+            pair(v[0][RL / 2], self, w2_at(one, RL / 2), h / 2);
+          }
+          // butterfly NS / 2: output r pairs with RL - 1 - r
+          const C w2h = omega2[NS / 2];
+#pragma unroll
+          for (int r = 0; r < RL / 2; ++r) pair(v[B / 2][r], v[B / 2][RL - 1 - r], w2_at(w2h, r), NS / 2 + r * NS);
+        } else {
+          const C w2j = omega2[jb[q]];
+#pragma unroll
+          for (int r = 0; r < RL; ++r) pair(v[q][r], v[q + B / 2][RL - 1 - r], w2_at(w2j, r), jb[q] + r * NS);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < B; ++q) {
+      dft_r<C, RL, true>(v[q]);
+      C w[RL];
+      stage_twiddles<C, RL, true>(tw, jb[q], w);
+      C* dst = col + P::at(jb[q]);
+      dst[0] = v[q][0];
+#pragma unroll
+      for (int r = 1; r < RL; ++r) dst[r * (NS + NS / 16)] = cmul(v[q][r], w[r]);
+    }
+    __syncthreads();
+  }
+  // ---- inverse: the middle stages' adjoints, then the first stage's into global memory
+  StagesAdj<C, FFT_EPT, LOGH, 16, LOGH - 4 - LOGRL, HP, NT>::run(s, tw);
+  {
+    const int cc = tid & (CPB - 1), j = tid >> logc, k = k0 + cc;
+    const C* col = s + cc * HP;
+    C v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = col[17 * j + r];
+    dft_r<C, 16, true>(v);
+    const T inv_h = (T)1 / (T)h;
+    if (k < N) {
+#pragma unroll
+      for (int r = 0; r < 16; ++r) {
+        const int p = j + r * (h / 16), row = r < 8 ? 2 * p : 2 * (h - 1 - p) + 1;
+        half[row * N + k] = cscale(v[r], inv_h);
       }
     }
   }
@@ -1600,6 +1816,7 @@ struct Tables {
   cplx<T>* post = nullptr;    // N entries e^(-2 pi i k / w)
   cplx<T>* tw_col = nullptr;  // h entries e^(-2 pi i t / h)
   cplx<T>* omega = nullptr;   // h entries e^(-i pi m / 2h)
+  cplx<T>* omega2 = nullptr;  // h entries e^(-i pi m / h)
   T* lx = nullptr;            // N + 1 entries 2 cos(2 pi k / w) - 2
   T* ly = nullptr;            // h entries 2 cos(pi m / h) - 2
 };
@@ -1662,6 +1879,9 @@ struct dt_flex {
   // test support: DT_STENCIL_WAIT_GIVE_UP=1 at create makes the TMA stencil's tile waits give up
   // without testing their barrier, so the solve takes the path of a wait that ran out
   int wait_give_up = 0;
+  // the column pass with its divide in registers (k_cols_fused) where the length allows;
+  // DT_COLS_FUSED=0 at create keeps k_cols everywhere (the same values, for comparison)
+  bool cols_fused = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
@@ -1707,7 +1927,7 @@ static dt_status dalloc(dt_flex* s, T** p, size_t count) {
 template <class T>
 static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
   int N = s->N, h = s->h, w = s->w;
-  std::vector<cplx<T>> a(N), b(N), c(h), o(h);
+  std::vector<cplx<T>> a(N), b(N), c(h), o(h), o2(h);
   std::vector<T> lx(N + 1), ly(h);
   for (int t = 0; t < N; ++t) {
     long double ang = -2.0L * PI_L * t / N;
@@ -1720,6 +1940,8 @@ static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
     c[t] = mk<cplx<T>>((T)cosl(ang), (T)sinl(ang));
     long double ang2 = -PI_L * t / (2.0L * h);
     o[t] = mk<cplx<T>>((T)cosl(ang2), (T)sinl(ang2));
+    long double ang3 = -PI_L * t / h;
+    o2[t] = mk<cplx<T>>((T)cosl(ang3), (T)sinl(ang3));
   }
   // the Laplacian's symbols as the reference forms them (flexure.rs:1145-1150), in double
   for (int k = 0; k <= N; ++k) lx[k] = (T)(2.0 * std::cos(6.283185307179586476925286766559 * (double)k / (double)w) - 2.0);
@@ -1728,12 +1950,14 @@ static dt_status make_tables(dt_flex* s, Tables<T>& tb) {
   DT_TRY(dalloc(s, &tb.post, N));
   DT_TRY(dalloc(s, &tb.tw_col, h));
   DT_TRY(dalloc(s, &tb.omega, h));
+  DT_TRY(dalloc(s, &tb.omega2, h));
   DT_TRY(dalloc(s, &tb.lx, N + 1));
   DT_TRY(dalloc(s, &tb.ly, h));
   DT_CUDA(cudaMemcpy(tb.tw_row, a.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
   DT_CUDA(cudaMemcpy(tb.post, b.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
   DT_CUDA(cudaMemcpy(tb.tw_col, c.data(), h * sizeof(cplx<T>), cudaMemcpyHostToDevice));
   DT_CUDA(cudaMemcpy(tb.omega, o.data(), h * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+  DT_CUDA(cudaMemcpy(tb.omega2, o2.data(), h * sizeof(cplx<T>), cudaMemcpyHostToDevice));
   DT_CUDA(cudaMemcpy(tb.lx, lx.data(), (N + 1) * sizeof(T), cudaMemcpyHostToDevice));
   DT_CUDA(cudaMemcpy(tb.ly, ly.data(), h * sizeof(T), cudaMemcpyHostToDevice));
   return DT_OK;
@@ -2024,6 +2248,14 @@ static void launch_apply(dt_flex* s, int mode, const T* v, const T* J, const T* 
   }
 }
 
+// Whether the column pass of length 2^logh runs k_cols_fused: FP32, a last radix below 16, and
+// at least two columns a k_cols block (h <= 2048), so that the fused block of half as many
+// columns stays within 256 threads.
+template <class T>
+static constexpr bool cols_fusable(int logh) {
+  return sizeof(T) == 4 && logh >= 5 && logh <= 11 && logh % 4 != 0;
+}
+
 // Launch geometry of the transform kernels: rows (RB rows a block) and columns (CPB columns a
 // block), each thread FFT_EPT complex values, padded shared memory.
 struct FftGeo {
@@ -2040,7 +2272,8 @@ static FftGeo fft_geometry(const dt_flex* s) {
   g.rgrid = ceil_div(s->h, RB);
   g.rthreads = std::max(1, RB * N / FFT_EPT);
   g.rsmem = (size_t)RB * Pad<C>::len(N) * sizeof(C);
-  int cpb = cols_per_block(logh, (int)sizeof(C));
+  int cpb = s->cols_fused && cols_fusable<T>(logh) ? cols_per_block_fused(logh, (int)sizeof(C))
+                                                   : cols_per_block(logh, (int)sizeof(C));
   g.cgrid = ceil_div(N, cpb);
   g.cthreads = std::max(1, cpb * s->h / FFT_EPT);
   g.csmem = (size_t)cpb * col_pitch(s->h) * sizeof(C);
@@ -2052,7 +2285,8 @@ constexpr int FFT_LOGS = 14;  // lengths 1 .. 8192
 template <class T, bool W>
 using RowsFwdFn = void (*)(int, int, const T*, const T*, cplx<T>*, const cplx<T>*, const cplx<T>*, const Scalars*);
 template <class T>
-using ColsFn = void (*)(int, cplx<T>*, const cplx<T>*, const cplx<T>*, const T*, const T*, T, const Scalars*, int);
+using ColsFn = void (*)(int, cplx<T>*, const cplx<T>*, const cplx<T>*, const cplx<T>*, const T*, const T*, T, const Scalars*,
+                        int);
 template <class T>
 using RowsInvFn = void (*)(int, int, const cplx<T>*, T*, const T*, const T*, const cplx<T>*, const cplx<T>*, double*, Scalars*);
 
@@ -2061,10 +2295,19 @@ static RowsFwdFn<T, W> rows_fwd_fn(int logn, std::integer_sequence<int, L...>) {
   static const RowsFwdFn<T, W> table[] = {&k_rows_fwd<T, W, L>...};
   return table[logn];
 }
+// The column kernel for length 2^L: the fused form when its last radix is below 16 (and
+// `fused`), else k_cols.
+template <class T, int L>
+static constexpr ColsFn<T> cols_kernel(bool fused) {
+  if constexpr (cols_fusable<T>(L))
+    return fused ? &k_cols_fused<T, L> : &k_cols<T, L>;
+  else
+    return &k_cols<T, L>;
+}
 template <class T, int... L>
-static ColsFn<T> cols_fn(int logh, std::integer_sequence<int, L...>) {
-  static const ColsFn<T> table[] = {&k_cols<T, L>...};
-  return table[logh];
+static ColsFn<T> cols_fn(int logh, std::integer_sequence<int, L...>, bool fused = true) {
+  static const ColsFn<T> table[2][sizeof...(L)] = {{cols_kernel<T, L>(false)...}, {cols_kernel<T, L>(true)...}};
+  return table[fused ? 1 : 0][logh];
 }
 template <class T, int MODE, int... L>
 static RowsInvFn<T> rows_inv_fn(int logn, std::integer_sequence<int, L...>) {
@@ -2089,7 +2332,8 @@ static void transform_smem_attributes() {
   for (int l = 0; l < FFT_LOGS; ++l) {
     cudaFuncSetAttribute(rows_fwd_fn<T, true>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     cudaFuncSetAttribute(rows_fwd_fn<T, false>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
-    cudaFuncSetAttribute(cols_fn<T>(l, LogSeq{}), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(cols_fn<T>(l, LogSeq{}, false), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    cudaFuncSetAttribute(cols_fn<T>(l, LogSeq{}, true), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     for (int m : {INV_STORE, INV_STORE_W, INV_STORE_DOT, INV_BANK})
       cudaFuncSetAttribute(rows_inv_for<T>(m, l), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
   }
@@ -2229,8 +2473,8 @@ static void launch_cols(dt_flex* s, Lane<T>& L, cplx<T>* half, const FftGeo& g, 
     for (int k = 0; k < 5; ++k) counted();
     return;
   }
-  cols_fn<T>(ilog2(s->h), LogSeq{})<<<g.cgrid, g.cthreads, g.csmem, st>>>(s->N, half, L.tab.tw_col, L.tab.omega, L.tab.lx,
-                                                                          L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S, level);
+  cols_fn<T>(ilog2(s->h), LogSeq{}, s->cols_fused)<<<g.cgrid, g.cthreads, g.csmem, st>>>(
+      s->N, half, L.tab.tw_col, L.tab.omega, L.tab.omega2, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), S, level);
   counted();
 }
 template <class T>
@@ -2913,6 +3157,8 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   }
   s->own_stream = true;
   if (const char* e = getenv("DT_STENCIL_WAIT_GIVE_UP")) s->wait_give_up = e[0] == '1';
+  if (const char* e = getenv("DT_COLS_FUSED")) s->cols_fused = e[0] != '0';
+
   // RowMetric::block (flexure.rs:1000-1010): the block metric's couplings, for a height the
   // cosine transform does not take
   std::vector<double> block_a, block_b;
