@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -300,6 +301,11 @@ __global__ void k_mg_diag(DLevel<TM> c, TM omega) {
   }
 }
 
+// Products rounded on their own (never fused into an add): the cycle's kernels form the same
+// values whichever kernel runs them, as the reference forms them (no fused multiply-adds).
+__device__ __forceinline__ float mulr(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mulr(double a, double b) { return __dmul_rn(a, b); }
+
 // A z at a cell of a level, in the level's term order (multigrid.rs:202-240), reading z (+ the
 // coarse correction of each cell's parent when zc is given).
 template <class TM>
@@ -311,15 +317,15 @@ __device__ __forceinline__ TM mg_apply_at(const DLevel<TM>& L, const TM* __restr
     return v;
   };
   size_t c = (size_t)j * L.w + i, c0 = (size_t)j * L.w;
-  TM o = L.diag[c] * zat(i, j);
-  if (i + 1 < L.w) o -= L.east[c] * zat(i + 1, j);
-  if (i > 0) o -= L.east[c - 1] * zat(i - 1, j);
+  TM o = mulr(L.diag[c], zat(i, j));
+  if (i + 1 < L.w) o -= mulr(L.east[c], zat(i + 1, j));
+  if (i > 0) o -= mulr(L.east[c - 1], zat(i - 1, j));
   if (L.wrap) {
-    if (i == L.w - 1) o -= L.east[c] * zat(0, j);
-    if (i == 0) o -= L.east[c0 + L.w - 1] * zat(L.w - 1, j);
+    if (i == L.w - 1) o -= mulr(L.east[c], zat(0, j));
+    if (i == 0) o -= mulr(L.east[c0 + L.w - 1], zat(L.w - 1, j));
   }
-  if (j + 1 < L.h) o -= L.south[c] * zat(i, j + 1);
-  if (j > 0) o -= L.south[c - L.w] * zat(i, j - 1);
+  if (j + 1 < L.h) o -= mulr(L.south[c], zat(i, j + 1));
+  if (j > 0) o -= mulr(L.south[c - L.w], zat(i, j - 1));
   return o;
 }
 
@@ -344,16 +350,19 @@ __global__ void k_mg_sweep(DLevel<TM> L, const TM* __restrict__ zin, TM* __restr
 }
 
 // rc = sum over each 2 x 2 block of (r - A z) (multigrid.rs:332-356)
+template <class TM, class K>
+__device__ __forceinline__ void restrict_cell(const DLevel<TM>& L, const TM* __restrict__ z, const DLevel<TM>& C, K k) {
+  int ic = (int)(k % C.w), jc = (int)(k / C.w);
+  TM acc = 0;
+  for (int j = 2 * jc; j < min(2 * jc + 2, L.h); ++j)
+    for (int i = 2 * ic; i < min(2 * ic + 2, L.w); ++i) acc += L.r[(size_t)j * L.w + i] - mg_apply_at<TM>(L, z, nullptr, 0, i, j);
+  C.r[k] = acc;
+}
 template <class TM>
 __global__ void k_mg_restrict(DLevel<TM> L, const TM* __restrict__ z, DLevel<TM> C) {
   size_t nc = (size_t)C.w * C.h;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x) {
-    int ic = (int)(k % C.w), jc = (int)(k / C.w);
-    TM acc = 0;
-    for (int j = 2 * jc; j < min(2 * jc + 2, L.h); ++j)
-      for (int i = 2 * ic; i < min(2 * ic + 2, L.w); ++i) acc += L.r[(size_t)j * L.w + i] - mg_apply_at<TM>(L, z, nullptr, 0, i, j);
-    C.r[k] = acc;
-  }
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc; k += (size_t)gridDim.x * blockDim.x)
+    restrict_cell<TM>(L, z, C, k);
 }
 
 // The colour of a cell for the Gauss-Seidel sweeps: (i + j) % 2, and on a wrapping level of odd
@@ -365,32 +374,41 @@ __device__ __forceinline__ int gs_colour(int w, int wrap, int i, int j) {
 }
 inline int gs_colours(int w, int wrap) { return (wrap && (w & 1)) ? 4 : 2; }
 
-// One Gauss-Seidel pass over the cells of colour `colour`: z_c += (r - A z)_c / diag_c.
-// FIRST: z is taken as 0 where this pass has not written (the cycle's first sweep).
+// One Gauss-Seidel update of cell k = (i, j) of colour `colour`: z_c += (r - A z)_c / diag_c.
+// FIRST: z is taken as 0 where this sweep has not written (the cycle's first sweep).
+template <class TM, bool FIRST>
+__device__ __forceinline__ void gs_cell_at(const DLevel<TM>& L, TM* __restrict__ z, int colour, size_t k, int i, int j) {
+  // in the first forward sweep, cells of later colours still hold 0 (not yet written)
+  auto zat = [&](int ii, int jj) -> TM {
+    if (FIRST && gs_colour(L.w, L.wrap, ii, jj) >= colour) return (TM)0;
+    return z[(size_t)jj * L.w + ii];
+  };
+  size_t c = k, c0 = (size_t)j * L.w;
+  TM zk = FIRST ? (TM)0 : z[c];
+  TM o = mulr(L.diag[c], zk);
+  if (i + 1 < L.w) o -= mulr(L.east[c], zat(i + 1, j));
+  if (i > 0) o -= mulr(L.east[c - 1], zat(i - 1, j));
+  if (L.wrap) {
+    if (i == L.w - 1) o -= mulr(L.east[c], zat(0, j));
+    if (i == 0) o -= mulr(L.east[c0 + L.w - 1], zat(L.w - 1, j));
+  }
+  if (j + 1 < L.h) o -= mulr(L.south[c], zat(i, j + 1));
+  if (j > 0) o -= mulr(L.south[c - L.w], zat(i, j - 1));
+  z[c] = zk + mulr(L.r[c] - o, L.wd[c]);  // wd = 1 / diag on the Gauss-Seidel hierarchy
+}
+template <class TM, bool FIRST>
+__device__ __forceinline__ void gs_cell(const DLevel<TM>& L, TM* __restrict__ z, int colour, size_t k) {
+  gs_cell_at<TM, FIRST>(L, z, colour, k, (int)(k % L.w), (int)(k / L.w));
+}
+
+// One Gauss-Seidel pass over the cells of colour `colour`.
 template <class TM, bool FIRST>
 __global__ void k_mg_gs(DLevel<TM> L, TM* __restrict__ z, int colour) {
   size_t n = (size_t)L.w * L.h;
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
     int i = (int)(k % L.w), j = (int)(k / L.w);
-    int col = gs_colour(L.w, L.wrap, i, j);
-    if (col != colour) continue;
-    // in the first forward sweep, cells of later colours still hold 0 (not yet written)
-    auto zat = [&](int ii, int jj) -> TM {
-      if (FIRST && gs_colour(L.w, L.wrap, ii, jj) >= colour) return (TM)0;
-      return z[(size_t)jj * L.w + ii];
-    };
-    size_t c = k, c0 = (size_t)j * L.w;
-    TM zk = FIRST ? (TM)0 : z[c];
-    TM o = L.diag[c] * zk;
-    if (i + 1 < L.w) o -= L.east[c] * zat(i + 1, j);
-    if (i > 0) o -= L.east[c - 1] * zat(i - 1, j);
-    if (L.wrap) {
-      if (i == L.w - 1) o -= L.east[c] * zat(0, j);
-      if (i == 0) o -= L.east[c0 + L.w - 1] * zat(L.w - 1, j);
-    }
-    if (j + 1 < L.h) o -= L.south[c] * zat(i, j + 1);
-    if (j > 0) o -= L.south[c - L.w] * zat(i, j - 1);
-    z[c] = zk + (L.r[c] - o) / L.diag[c];
+    if (gs_colour(L.w, L.wrap, i, j) != colour) continue;
+    gs_cell<TM, FIRST>(L, z, colour, k);
   }
 }
 
@@ -406,9 +424,9 @@ __global__ void k_mg_prolong(DLevel<TM> L, TM* __restrict__ z, const TM* __restr
 
 // The coarsest level in one block (at most 128 cells): KIND 0 the reference's first sweep and
 // 15 damped Jacobi sweeps (multigrid.rs:504-512); KIND 1 eight forward and eight backward
-// multi-colour Gauss-Seidel sweeps. Result in z.
+// multi-colour Gauss-Seidel sweeps. Result in z. Every thread of the block takes part.
 template <class TM, int KIND>
-__global__ void k_mg_coarsest(DLevel<TM> L, TM* __restrict__ z, int sweeps) {
+__device__ __forceinline__ void coarsest_solve(const DLevel<TM>& L, TM* __restrict__ z, int sweeps) {
   __shared__ TM sz[2][256];
   int n = L.w * L.h;
   int k = threadIdx.x;
@@ -438,7 +456,7 @@ __global__ void k_mg_coarsest(DLevel<TM> L, TM* __restrict__ z, int sweeps) {
           int i = k % L.w, j = k / L.w;
           if (gs_colour(L.w, L.wrap, i, j) == colour) {
             TM az = mg_apply_at<TM>(L, sz[0], nullptr, 0, i, j);
-            sz[0][k] = sz[0][k] + (L.r[k] - az) / L.diag[k];
+            sz[0][k] = sz[0][k] + mulr(L.r[k] - az, L.wd[k]);
           }
         }
         __syncthreads();
@@ -446,6 +464,238 @@ __global__ void k_mg_coarsest(DLevel<TM> L, TM* __restrict__ z, int sweeps) {
     }
     if (k < n) z[k] = sz[0][k];
   }
+}
+template <class TM, int KIND>
+__global__ void k_mg_coarsest(DLevel<TM> L, TM* __restrict__ z, int sweeps) {
+  coarsest_solve<TM, KIND>(L, z, sweeps);
+}
+
+// The Gauss-Seidel V-cycle's part from a level of at most MG_BLOCK_CELLS cells down, in one
+// block of 1024 threads (the coarsest level on the first 128): the same passes in the same order as the separate launches (pre-sweeps,
+// restriction, the coarser levels, prolongation, post-sweeps), a block barrier where a launch
+// ended, so the same values. The levels' arrays are staged in shared memory first (off[q]: the
+// level's first cell there, six arrays of `total` cells); the top level's z goes back at the end.
+constexpr int MG_BLOCK_LEVELS = 8;
+template <class TM>
+struct MgChain {
+  DLevel<TM> lv[MG_BLOCK_LEVELS];
+  int off[MG_BLOCK_LEVELS];
+  int count, total;
+};
+template <class TM>
+__global__ void __launch_bounds__(1024) k_mg_coarse_rb(MgChain<TM> g, int nu, int coarse_sweeps) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+  extern __shared__ __align__(16) unsigned char mg_chain_smem[];
+  TM* const sbase = reinterpret_cast<TM*>(mg_chain_smem);
+  // level q as staged in shared memory (built in registers where it is used)
+  auto sl = [&](int q) {
+    DLevel<TM> L = g.lv[q];
+    L.z = sbase + 0 * g.total + g.off[q];
+    L.r = sbase + 1 * g.total + g.off[q];
+    L.diag = sbase + 2 * g.total + g.off[q];
+    L.wd = sbase + 3 * g.total + g.off[q];
+    L.east = sbase + 4 * g.total + g.off[q];
+    L.south = sbase + 5 * g.total + g.off[q];
+    return L;
+  };
+  for (int q = 0; q < g.count; ++q) {
+    const DLevel<TM> L = sl(q);
+    const DLevel<TM>& G = g.lv[q];
+    const int n = G.w * G.h;
+    for (int k = tid; k < n; k += nt) {
+      L.z[k] = (TM)0;
+      L.r[k] = q == 0 ? G.r[k] : (TM)0;
+      L.diag[k] = G.diag[k];
+      L.wd[k] = G.wd[k];
+      L.east[k] = G.east[k];
+      L.south[k] = G.south[k];
+    }
+  }
+  __syncthreads();
+  for (int q = 0; q + 1 < g.count; ++q) {
+    const DLevel<TM> L = sl(q);
+    const int n = L.w * L.h;
+    const int ncol = (L.wrap && (L.w & 1)) ? 4 : 2;
+    for (int sweep = 0; sweep < nu; ++sweep)
+      for (int c = 0; c < ncol; ++c) {
+        for (int k = tid; k < n; k += nt) {
+          const int j = k / L.w, i = k - j * L.w;
+          if (gs_colour(L.w, L.wrap, i, j) != c) continue;
+          if (sweep == 0)
+            gs_cell_at<TM, true>(L, L.z, c, k, i, j);
+          else
+            gs_cell_at<TM, false>(L, L.z, c, k, i, j);
+        }
+        __syncthreads();
+      }
+    const DLevel<TM> C = sl(q + 1);
+    for (int k = tid; k < C.w * C.h; k += nt) restrict_cell<TM>(L, L.z, C, k);
+    __syncthreads();
+  }
+  {
+    // the coarsest level (at most 128 cells, one a thread) on the block's first 128 threads:
+    // coarsest_solve's Gauss-Seidel passes in place on the staged z, with a barrier of those
+    // threads between passes
+    const DLevel<TM> L = sl(g.count - 1);
+    if (tid < 128) {
+      const int n = L.w * L.h;
+      const int ncol = (L.wrap && (L.w & 1)) ? 4 : 2;
+      const int j = tid / L.w, i = tid - j * L.w;
+      for (int pass = 0; pass < 2 * coarse_sweeps; ++pass) {
+        const bool forward = pass < coarse_sweeps;
+        for (int q = 0; q < ncol; ++q) {
+          const int colour = forward ? q : ncol - 1 - q;
+          if (tid < n && gs_colour(L.w, L.wrap, i, j) == colour) {
+            TM az = mg_apply_at<TM>(L, L.z, nullptr, 0, i, j);
+            L.z[tid] = L.z[tid] + mulr(L.r[tid] - az, L.wd[tid]);
+          }
+          asm volatile("bar.sync 1, 128;" ::: "memory");
+        }
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = g.count - 2; q >= 0; --q) {
+    const DLevel<TM> L = sl(q), C = sl(q + 1);
+    const int n = L.w * L.h;
+    const int ncol = (L.wrap && (L.w & 1)) ? 4 : 2;
+    for (int k = tid; k < n; k += nt) {
+      const int j = k / L.w, i = k - j * L.w;
+      L.z[k] += C.z[(j / 2) * C.w + i / 2];
+    }
+    __syncthreads();
+    for (int sweep = 0; sweep < nu; ++sweep)
+      for (int c = ncol - 1; c >= 0; --c) {
+        for (int k = tid; k < n; k += nt) {
+          const int j = k / L.w, i = k - j * L.w;
+          if (gs_colour(L.w, L.wrap, i, j) != c) continue;
+          gs_cell_at<TM, false>(L, L.z, c, k, i, j);
+        }
+        __syncthreads();
+      }
+  }
+  {
+    const DLevel<TM> L = sl(0);
+    for (int k = tid; k < L.w * L.h; k += nt) g.lv[0].z[k] = L.z[k];
+  }
+}
+
+// Two red-black Gauss-Seidel sweeps (four colour passes) of a level in one launch, over tiles of
+// MG_TX x MG_TY cells staged in shared memory with a halo: pass p updates its colour on the tile
+// and the rings around it that the later passes read, so the tile's cells end with the values
+// four separate passes give (temporal blocking; each update is gs_cell's, term for term).
+//   PRE   the pre-smoothing: z from 0, colours 0, 1, 0, 1; then the residual r - A z on the
+//         tile and its 2 x 2 sums into the coarser level's r (k_mg_restrict's arithmetic), so
+//         the restriction needs no launch of its own (halo 5: z is final one ring out);
+//   !PRE  the post-smoothing: z += P zc (the coarse correction, piecewise constant), then
+//         colours 1, 0, 1, 0 (halo 4).
+// For levels of two colours (no wrap, or an even width) at least MG_TX + 10 cells wide, so that
+// no cell sits twice in a tile. Shared memory holds the region in red-black order, so that a
+// colour pass reads and writes consecutive words with no idle lanes.
+constexpr int MG_TX = 32, MG_TY = 16;
+template <class TM, bool PRE>
+__global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, const TM* __restrict__ zc) {
+  constexpr int HALO = PRE ? 5 : 4;
+  constexpr int SX = MG_TX + 2 * HALO, SY = MG_TY + 2 * HALO;
+  constexpr int HX = SX / 2, NC = HX * SY;  // a colour's cells of a row, of the region
+  static_assert(SX % 2 == 0, "rb2: even rows");
+  // red-black layout: cell (lx, ly) of colour k = (i0 + lx + j0 + ly) & 1 at a[k][ly * HX + lx / 2]
+  extern __shared__ __align__(16) unsigned char mg_smem[];
+  TM* const base = reinterpret_cast<TM*>(mg_smem);
+  // array a (0 z, 1 r, 2 diag, 3 wd, 4 east, 5 south) of colour k
+  auto A = [&](int a, int k) { return base + (2 * a + k) * NC; };
+  const int i0 = blockIdx.x * MG_TX - HALO, j0 = blockIdx.y * MG_TY - HALO;
+  const int off = (i0 + j0) & 1;
+  const int tid = threadIdx.x;
+  const int w = L.w, h = L.h;
+  auto gcol = [&](int lx) {
+    int gi = i0 + lx;
+    if (L.wrap) gi = gi < 0 ? gi + w : (gi >= w ? gi - w : gi);
+    return gi;
+  };
+  for (int e = tid; e < SX * SY; e += 256) {
+    const int ly = e / SX, lx = e - ly * SX;
+    const int gi = gcol(lx), gj = j0 + ly;
+    if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
+    const int k = (lx + ly + off) & 1, q = ly * HX + (lx >> 1);
+    const size_t c = (size_t)gj * w + gi;
+    TM zv = PRE ? (TM)0 : L.z[c];
+    if (!PRE) zv += zc[(size_t)(gj / 2) * C.w + gi / 2];
+    A(0, k)[q] = zv;
+    A(1, k)[q] = L.r[c];
+    A(2, k)[q] = L.diag[c];
+    A(3, k)[q] = L.wd[c];
+    A(4, k)[q] = L.east[c];
+    A(5, k)[q] = L.south[c];
+  }
+  __syncthreads();
+  // pass p updates its colour at least p + 1 cells from the region's border: a row's cells of
+  // one colour are consecutive, so consecutive threads take consecutive cells
+#pragma unroll
+  for (int pass = 0; pass < 4; ++pass) {
+    const int k = PRE ? (pass & 1) : 1 - (pass & 1), o_ = 1 - k;
+    const int lo = pass + 1, RW = SX - 2 * lo, RH = SY - 2 * lo, HW = RW / 2;
+    const TM* zo = A(0, o_);
+    for (int idx = tid; idx < RH * HW; idx += 256) {
+      const int ly = lo + idx / HW;
+      const int p = (k + ly + off) & 1;  // the parity of lx of colour k on this row
+      const int lx = lo + ((p - lo) & 1) + 2 * (idx - (ly - lo) * HW);
+      const int gi = gcol(lx), gj = j0 + ly;
+      if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
+      const int q = ly * HX + (lx >> 1);
+      const int qw = ly * HX + ((lx - 1) >> 1), qe = ly * HX + ((lx + 1) >> 1);  // the other colour's
+      TM* const zs = A(0, k);
+      const TM zk = zs[q];
+      const TM ec = A(4, k)[q], ew = A(4, o_)[qw];
+      TM o = mulr(A(2, k)[q], zk);
+      if (gi + 1 < w) o -= mulr(ec, zo[qe]);
+      if (gi > 0) o -= mulr(ew, zo[qw]);
+      if (L.wrap) {
+        if (gi == w - 1) o -= mulr(ec, zo[qe]);
+        if (gi == 0) o -= mulr(ew, zo[qw]);
+      }
+      if (gj + 1 < h) o -= mulr(A(5, k)[q], zo[q + HX]);
+      if (gj > 0) o -= mulr(A(5, o_)[q - HX], zo[q - HX]);
+      zs[q] = zk + mulr(A(1, k)[q] - o, A(3, k)[q]);
+    }
+    __syncthreads();
+  }
+  auto at = [&](int a, int lx, int ly) -> TM { return A(a, (lx + ly + off) & 1)[ly * HX + (lx >> 1)]; };
+  if (PRE) {
+    // the residual of the tile's cells (mg_apply_at's order) summed over 2 x 2 blocks into C.r,
+    // in k_mg_restrict's order
+    constexpr int CX = MG_TX / 2, CY = MG_TY / 2;
+    if (tid < CX * CY) {
+      const int ic = blockIdx.x * CX + tid % CX, jc = blockIdx.y * CY + tid / CX;
+      if (ic < C.w && jc < C.h) {
+        TM acc = 0;
+        for (int j = 2 * jc; j < min(2 * jc + 2, h); ++j)
+          for (int i = 2 * ic; i < min(2 * ic + 2, w); ++i) {
+            const int lx = i - i0, ly = j - j0;
+            TM o = mulr(at(2, lx, ly), at(0, lx, ly));
+            if (i + 1 < w) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
+            if (i > 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
+            if (L.wrap) {
+              if (i == w - 1) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
+              if (i == 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
+            }
+            if (j + 1 < h) o -= mulr(at(5, lx, ly), at(0, lx, ly + 1));
+            if (j > 0) o -= mulr(at(5, lx, ly - 1), at(0, lx, ly - 1));
+            acc += at(1, lx, ly) - o;
+          }
+        C.r[(size_t)jc * C.w + ic] = acc;
+      }
+    }
+  }
+  for (int e = tid; e < MG_TX * MG_TY; e += 256) {
+    const int ly = HALO + e / MG_TX, lx = HALO + e % MG_TX;
+    const int gi = i0 + lx, gj = j0 + ly;
+    if (gi < w && gj < h) L.z[(size_t)gj * w + gi] = at(0, lx, ly);
+  }
+}
+template <class TM, bool PRE>
+constexpr size_t mg_rb2_smem() {
+  return (size_t)6 * (MG_TX + 2 * (PRE ? 5 : 4)) * (MG_TY + 2 * (PRE ? 5 : 4)) * sizeof(TM);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -523,93 +773,6 @@ __global__ void k_lod_rows(int w, int h, int wrap, double* __restrict__ hf, cons
   }
 }
 
-// The LOD row pass for wrapping rows with w > 2, on transposed arrays (element (j, i) at i h + j):
-// thread j walks row j, consecutive threads take consecutive rows, so every step reads and writes
-// contiguous words. The arithmetic is k_lod_rows', operation for operation: the coefficients
-// computed on the fly from kd, Sherman-Morrison's two right-hand sides in one elimination
-// (diffusion.rs:1048-1071, :370-419). cT, xT, zT: scratch of w h values; the result into outT.
-__global__ void __launch_bounds__(32) k_lod_rows_wrap_t(int w, int h, double dtdx2, const double* __restrict__ kdT,
-                                                      const double* __restrict__ hfT, double* __restrict__ cT,
-                                                      double* __restrict__ xT, double* __restrict__ zT,
-                                                      double* __restrict__ fact_out) {
-  constexpr int RB = 16;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= h) return;
-  auto at = [&](int i) { return (size_t)i * h + j; };
-  const double kfirst = kdT[at(0)], klast = kdT[at(w - 1)];
-  const double fw = 0.5 * (klast + kfirst) * dtdx2;  // face(w - 1), across the seam
-  // row 0: west = face(w - 1), east = face(0)
-  double kprev = kfirst;
-  const double east0 = 0.5 * (kfirst + kdT[at(1)]) * dtdx2;
-  const double di0 = 1.0 + fw + east0;
-  const double alpha = -fw, beta = -fw, gamma = -di0;  // up[w-1], lo[0], and -di[0]
-  double bt = di0 - gamma;
-  double xp = hfT[at(0)] / bt, zp = gamma / bt;
-  xT[at(0)] = xp;
-  zT[at(0)] = zp;
-  double west = east0;  // face(i - 1) for the next row
-  kprev = kdT[at(1)];
-  for (int i0 = 1; i0 < w; i0 += RB) {
-    double kn[RB], hv[RB];
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int i = min(i0 + u, w - 1);
-      kn[u] = i + 1 < w ? kdT[at(i + 1)] : 0.0;
-      hv[u] = hfT[at(i)];
-    }
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int i = i0 + u;
-      if (i >= w) break;
-      const double east = i + 1 < w ? 0.5 * (kprev + kn[u]) * dtdx2 : fw;
-      kprev = kn[u];
-      const double lo = -west, upp = -west;  // lo[i] = -face(i - 1) = up[i - 1]
-      double di = 1.0 + west + east;
-      if (i == w - 1) di = di - alpha * beta / gamma;
-      const double c = upp / bt;
-      bt = di - lo * c;
-      xp = (hv[u] - lo * xp) / bt;
-      zp = ((i == w - 1 ? alpha : 0.0) - lo * zp) / bt;
-      cT[at(i)] = c;
-      xT[at(i)] = xp;
-      zT[at(i)] = zp;
-      west = east;
-    }
-  }
-  // back substitution, both right-hand sides
-  double xn = xT[at(w - 1)], zn = zT[at(w - 1)];
-  const double xlast = xn, zlast = zn;
-  for (int i0 = w - 2; i0 >= 0; i0 -= RB) {
-    double cn[RB], xv[RB], zv[RB];
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int i = max(i0 - u, 0);
-      cn[u] = cT[at(i + 1)];
-      xv[u] = xT[at(i)];
-      zv[u] = zT[at(i)];
-    }
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int i = i0 - u;
-      if (i < 0) break;
-      xn = xv[u] - cn[u] * xn;
-      zn = zv[u] - cn[u] * zn;
-      xT[at(i)] = xn;
-      zT[at(i)] = zn;
-    }
-  }
-  // Sherman-Morrison's factor; k_lod_rows_combine forms x - fact z with every thread of the GPU
-  fact_out[j] = (xn + beta * xlast / gamma) / (1.0 + zn + beta * zlast / gamma);
-}
-
-// out = x - fact z per cell of the transposed rows (element (j, i) at i h + j)
-__global__ void k_lod_rows_combine(int w, int h, const double* __restrict__ xT, const double* __restrict__ zT,
-                                   const double* __restrict__ fact, double* __restrict__ outT) {
-  const size_t n = (size_t)w * h;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
-    outT[k] = xT[k] - fact[k % h] * zT[k];
-}
-
 // 32 x 32 tiles through shared memory: out (cols x rows) = the transpose of in (rows x cols)
 __global__ void k_transpose(int rows, int cols, const double* __restrict__ in, double* __restrict__ out) {
   __shared__ double tile[32][33];
@@ -625,61 +788,175 @@ __global__ void k_transpose(int rows, int cols, const double* __restrict__ in, d
   }
 }
 
-// The LOD column pass (rows closed, diffusion.rs:420-489): thread i walks column i (consecutive
-// threads, consecutive words), the tridiagonal (1 + north + south, -north, -south) built on the
-// fly and solved by Thomas (diffusion.rs:1029-1046) in place; the Thomas coefficients into cs.
-__global__ void __launch_bounds__(32) k_lod_cols_fast(int w, int h, double* __restrict__ hf, const double* __restrict__ kd,
-                                                    double dtdx2, double* __restrict__ cs) {
-  constexpr int RB = 16;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= w) return;
-  auto at = [&](int j) { return (size_t)j * w + i; };
-  double kcur = kd[at(0)];
-  double south = h > 1 ? 0.5 * (kcur + kd[at(1)]) * dtdx2 : 0.0;
-  double bt = 1.0 + 0.0 + south;  // di[0] = 1 + north + south with north = 0
-  double bp = hf[at(0)] / bt;
-  hf[at(0)] = bp;
-  double north = south;
-  if (h > 1) kcur = kd[at(1)];
-  for (int j0 = 1; j0 < h; j0 += RB) {
-    double kn[RB], hv[RB];
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int j = min(j0 + u, h - 1);
-      kn[u] = j + 1 < h ? kd[at(j + 1)] : 0.0;
-      hv[u] = hf[at(j)];
-    }
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int j = j0 + u;
-      if (j >= h) break;
-      const double s2 = j + 1 < h ? 0.5 * (kcur + kn[u]) * dtdx2 : 0.0;
-      kcur = kn[u];
-      const double lo = -north, upp = -north;  // lo[j] = -face(j - 1) = up[j - 1]
-      const double di = 1.0 + north + s2;
-      const double c = upp / bt;
-      bt = di - lo * c;
-      bp = (hv[u] - lo * bp) / bt;
-      cs[at(j)] = c;
-      hf[at(j)] = bp;
-      north = s2;
-    }
+// The LOD passes as partitioned tridiagonal solves: L independent lines of n unknowns, stored
+// line-fastest (element (l, i) at i L + l: the rows on transposed copies, the columns as they lie),
+// each split into chunks of LOD_CHUNK unknowns solved in parallel (L x chunks threads instead of
+// L): a thread eliminates its chunk (Thomas, diffusion.rs:1029-1046) for the right-hand sides
+// and for the two unit couplings to the unknowns just outside the chunk, y = p + q y_(s-1) +
+// r y_e; one thread a line then solves the chunks' end values from those relations (a two-term
+// recurrence, forward and back), and every cell forms its y. The coefficients are the LOD's
+// (diffusion.rs:370-489), formed on the fly from kd: faces 0.5 (k_i + k_(i+1)) dt / dx^2 and
+// diagonal (1 + west) + east. ROWS: the periodic rows through Sherman-Morrison (diffusion.rs:
+// 1048-1071): the system with the corners folded into the first and last diagonal, solved for b
+// and for u = (gamma, 0, .., 0, alpha), then x - fact z. Columns: rows closed, one right-hand side.
+constexpr int LOD_CHUNK = 64;
+template <bool ROWS>
+struct LodLine {
+  const double* kd;
+  int L, n, l;
+  double dtdx2;
+  __device__ double K(int i) const { return kd[(size_t)i * L + l]; }
+  // the face between positions i and i + 1 (across the seam for the rows' last one)
+  __device__ double face(int i) const {
+    if (i + 1 < n) return 0.5 * (K(i) + K(i + 1)) * dtdx2;
+    return ROWS ? 0.5 * (K(n - 1) + K(0)) * dtdx2 : 0.0;
   }
-  double bn = bp;
-  for (int j0 = h - 2; j0 >= 0; j0 -= RB) {
-    double cn[RB], bv[RB];
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int j = max(j0 - u, 0);
-      cn[u] = cs[at(j + 1)];
-      bv[u] = hf[at(j)];
+};
+
+template <bool ROWS>
+__global__ void __launch_bounds__(128) k_lod_chunks(int L, int n, int P, double dtdx2, const double* __restrict__ kd,
+                                                    double* __restrict__ p0, double* __restrict__ p1, double* __restrict__ q,
+                                                    double* __restrict__ r, double* __restrict__ c, double* __restrict__ edge) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L * P) return;
+  const int l = t % L, k = t / L;
+  const int s = k * LOD_CHUNK, e = min(s + LOD_CHUNK, n);
+  const LodLine<ROWS> ln{kd, L, n, l, dtdx2};
+  auto at = [&](int i) { return (size_t)i * L + l; };
+  // rows: the folded corners (k_lod_rows' alpha = up[n-1], beta = lo[0], gamma = -di[0])
+  double fw = 0.0, alpha = 0.0, beta = 0.0, gamma = -1.0;
+  if (ROWS) {
+    fw = ln.face(n - 1);
+    const double di0 = 1.0 + fw + ln.face(0);
+    alpha = -fw;
+    beta = -fw;
+    gamma = -di0;
+  }
+  double west = s == 0 ? (ROWS ? fw : 0.0) : ln.face(s - 1);
+  double bt = 1.0, cprev = 0.0, pv0 = 0.0, pv1 = 0.0, qv = 0.0, rv = 0.0;
+  for (int i = s; i < e; ++i) {
+    const double east = ln.face(i);
+    double di = 1.0 + west + east;
+    if (ROWS && i == 0) di = di - gamma;
+    if (ROWS && i == n - 1) di = di - alpha * beta / gamma;
+    const double lo = i == 0 ? 0.0 : -west;
+    const double up = (ROWS && i == n - 1) ? 0.0 : -east;
+    const double b0 = p0[at(i)];
+    const double b1 = ROWS ? (i == 0 ? gamma : (i == n - 1 ? alpha : 0.0)) : 0.0;
+    const double rr = i == e - 1 ? -up : 0.0;
+    if (i == s) {
+      bt = di;
+      pv0 = b0 / bt;
+      pv1 = b1 / bt;
+      qv = -lo / bt;
+      rv = rr / bt;
+    } else {
+      bt = di - lo * cprev;
+      pv0 = (b0 - lo * pv0) / bt;
+      pv1 = (b1 - lo * pv1) / bt;
+      qv = (0.0 - lo * qv) / bt;
+      rv = (rr - lo * rv) / bt;
     }
-#pragma unroll
-    for (int u = 0; u < RB; ++u) {
-      const int j = j0 - u;
-      if (j < 0) break;
-      bn = bv[u] - cn[u] * bn;
-      hf[at(j)] = bn;
+    cprev = up / bt;
+    c[at(i)] = cprev;
+    p0[at(i)] = pv0;
+    if (ROWS) p1[at(i)] = pv1;
+    q[at(i)] = qv;
+    r[at(i)] = rv;
+    west = east;
+  }
+  // back substitution inside the chunk: y_i -= c_i y_(i+1)
+  const double e0 = pv0, e1 = pv1, eq = qv, er = rv;  // the last position's values are final
+  for (int i = e - 2; i >= s; --i) {
+    const double ci = c[at(i)];
+    pv0 = p0[at(i)] - ci * pv0;
+    p0[at(i)] = pv0;
+    if (ROWS) {
+      pv1 = p1[at(i)] - ci * pv1;
+      p1[at(i)] = pv1;
+    }
+    qv = q[at(i)] - ci * qv;
+    q[at(i)] = qv;
+    rv = r[at(i)] - ci * rv;
+    r[at(i)] = rv;
+  }
+  double* ed = edge + (size_t)t * 8;  // (k L + l) * 8: first position, then last
+  ed[0] = pv0;
+  ed[1] = pv1;
+  ed[2] = qv;
+  ed[3] = rv;
+  ed[4] = e0;
+  ed[5] = e1;
+  ed[6] = eq;
+  ed[7] = er;
+}
+
+// One thread a line: the chunks' first (A_k) and last (B_k) values from A_k = pA + qA B_(k-1) +
+// rA A_(k+1), B_k = pB + qB B_(k-1) + rB A_(k+1): forward, B_(k-1) = g + h A_k; back from A_P = 0.
+// Written over the edge record's p entries (A_k into [0], [1], B_k into [4], [5]); ROWS: fact of
+// the line into fact[l].
+template <bool ROWS>
+__global__ void __launch_bounds__(128) k_lod_reduce(int L, int n, int P, double dtdx2, const double* __restrict__ kd,
+                                                    double* __restrict__ edge, double* __restrict__ al,
+                                                    double* __restrict__ fact) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L) return;
+  constexpr int NR = ROWS ? 2 : 1;
+  double A0[NR], Bl[NR];
+  for (int rhs = 0; rhs < NR; ++rhs) {
+    double g = 0.0, hh = 0.0;
+    for (int k = 0; k < P; ++k) {
+      const double* ed = edge + ((size_t)k * L + l) * 8;
+      const double pA = ed[rhs], qA = ed[2], rA = ed[3], pB = ed[4 + rhs], qB = ed[6], rB = ed[7];
+      const double d = 1.0 - qA * hh;
+      const double a = (pA + qA * g) / d, be = rA / d;
+      // scratch for the way back: alpha, beta, g, h of chunk k
+      double* sk = al + ((size_t)k * L + l) * 4;
+      sk[0] = a;
+      sk[1] = be;
+      g = pB + qB * g + qB * hh * a;
+      hh = qB * hh * be + rB;
+      sk[2] = g;
+      sk[3] = hh;
+    }
+    double An = 0.0;
+    for (int k = P - 1; k >= 0; --k) {
+      const double* sk = al + ((size_t)k * L + l) * 4;
+      const double A = sk[0] + sk[1] * An, B = sk[2] + sk[3] * An;
+      double* ed = edge + ((size_t)k * L + l) * 8;
+      ed[rhs] = A;
+      ed[4 + rhs] = B;
+      if (k == P - 1) Bl[rhs] = B;
+      An = A;
+    }
+    A0[rhs] = An;
+  }
+  if (ROWS) {
+    const LodLine<true> ln{kd, L, n, l, dtdx2};
+    const double fw = ln.face(n - 1);
+    const double beta = -fw, gamma = -(1.0 + fw + ln.face(0));
+    fact[l] = (A0[0] + beta * Bl[0] / gamma) / (1.0 + A0[1] + beta * Bl[1] / gamma);
+  }
+}
+
+// Every cell: y = p + q B_(k-1) + r A_(k+1) per right-hand side; ROWS: out = y_b - fact y_u.
+// The result over p0.
+template <bool ROWS>
+__global__ void __launch_bounds__(256) k_lod_finish(int L, int n, int P, double* __restrict__ p0, const double* __restrict__ p1,
+                                                    const double* __restrict__ q, const double* __restrict__ r,
+                                                    const double* __restrict__ edge, const double* __restrict__ fact) {
+  const size_t total = (size_t)L * n;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int l = (int)(t % L), i = (int)(t / L), k = i / LOD_CHUNK;
+    const double* em = k > 0 ? edge + ((size_t)(k - 1) * L + l) * 8 : nullptr;
+    const double* ep = k + 1 < P ? edge + ((size_t)(k + 1) * L + l) * 8 : nullptr;
+    const double qv = q[t], rv = r[t];
+    const double y0 = p0[t] + qv * (em ? em[4] : 0.0) + rv * (ep ? ep[0] : 0.0);
+    if (ROWS) {
+      const double y1 = p1[t] + qv * (em ? em[5] : 0.0) + rv * (ep ? ep[1] : 0.0);
+      p0[t] = y0 - fact[l] * y1;
+    } else {
+      p0[t] = y0;
     }
   }
 }
@@ -766,6 +1043,7 @@ static const int COARSEST = 64;     // multigrid.rs:54
 static const int COARSE_SWEEPS = 16;  // multigrid.rs:56
 static const int COARSEST_GS = 128;   // the Gauss-Seidel cycle's coarsest level: 16 x 8 cells
 static const int COARSE_SWEEPS_GS = 8;
+static const int MG_BLOCK_CELLS = 2048;  // Gauss-Seidel levels this small run their part of the cycle in one block
 
 template <class TM>
 struct Hier {
@@ -796,13 +1074,16 @@ struct dt_diff {
   double *east = nullptr, *south = nullptr, *diag = nullptr;
   float *east32 = nullptr, *south32 = nullptr, *diag32 = nullptr;
   float *x32 = nullptr, *r32 = nullptr, *p32 = nullptr, *ap32 = nullptr;
-  double* lod[6] = {};
+  double* lod[7] = {};  // the LOD first guess's scratch (lod[6]: its chunks' end values)
   double* partials = nullptr;
   double* scale = nullptr;
   dt::DScalars *S64 = nullptr, *S32 = nullptr;
   dt::Hier<float> hf[2];
   dt::Hier<double> hd[2];
   dt::DGraph graph[3][2];
+  // the Gauss-Seidel cycle's fused kernels (k_mg_rb2, k_mg_coarse_rb); DT_MG_FUSED=0 at create
+  // keeps one launch per colour pass (the same values)
+  bool mg_fused = true;
 };
 
 namespace dt {
@@ -854,15 +1135,17 @@ static dt_status build_levels(dt_diff* s, Hier<TM>& H, int coarsest) {
 
 // Level coefficients for the current operator: the finest from the FP64 couplings, the rest by
 // aggregation.
+// wd: omega / diag for the damped-Jacobi cycle, 1 / diag for the Gauss-Seidel one.
 template <class TM>
-static void fill_levels(dt_diff* s, Hier<TM>& H, cudaStream_t st) {
+static void fill_levels(dt_diff* s, Hier<TM>& H, int kind, cudaStream_t st) {
   DLevel<TM>& f = H.lv[0];
-  k_mg_finest<TM><<<dgrid(s, s->n), 256, 0, st>>>(s->n, s->east, s->south, s->diag, (TM)OMEGA, f.east, f.south, f.diag, f.wd, f.mass);
+  const TM omega = kind == DT_CYCLE_JACOBI ? (TM)OMEGA : (TM)1;
+  k_mg_finest<TM><<<dgrid(s, s->n), 256, 0, st>>>(s->n, s->east, s->south, s->diag, omega, f.east, f.south, f.diag, f.wd, f.mass);
   count_launch();
   for (size_t l = 1; l < H.lv.size(); ++l) {
     size_t nc = (size_t)H.lv[l].w * H.lv[l].h;
     k_mg_coarsen<TM><<<dgrid(s, nc), 256, 0, st>>>(H.lv[l - 1], H.lv[l], (TM)SCALE);
-    k_mg_diag<TM><<<dgrid(s, nc), 256, 0, st>>>(H.lv[l], (TM)OMEGA);
+    k_mg_diag<TM><<<dgrid(s, nc), 256, 0, st>>>(H.lv[l], omega);
     count_launch();
     count_launch();
   }
@@ -909,6 +1192,37 @@ static TM* vcycle(dt_diff* s, Hier<TM>& H, size_t l, int kind, cudaStream_t st) 
   }
   // multi-colour Gauss-Seidel V(NU, NU): colours forward, coarse correction, colours backward
   int ncol = gs_colours(L.w, L.wrap);
+  if (s->mg_fused) {
+    // this level and every coarser one in one block, when it is small enough
+    if (n <= (size_t)MG_BLOCK_CELLS && H.lv.size() - l <= (size_t)MG_BLOCK_LEVELS) {
+      MgChain<TM> m{};
+      m.count = (int)(H.lv.size() - l);
+      m.total = 0;
+      for (int q = 0; q < m.count; ++q) {
+        m.lv[q] = H.lv[l + q];
+        m.off[q] = m.total;
+        m.total += H.lv[l + q].w * H.lv[l + q].h;
+      }
+      const size_t smem = (size_t)6 * m.total * sizeof(TM);
+      const DLevel<TM>& last = H.lv.back();
+      if (smem <= 200 * 1024 && last.w * last.h <= 128) {  // the coarsest takes one thread a cell of 128
+        k_mg_coarse_rb<TM><<<1, 1024, smem, st>>>(m, NU, COARSE_SWEEPS_GS);
+        count_launch();
+        return L.z;
+      }
+    }
+    // both sweeps of the smoothing in one launch over tiles, the restriction fused into the
+    // pre-smoothing (two-colour levels wide enough)
+    if (ncol == 2 && NU == 2 && L.w >= MG_TX + 10) {
+      const dim3 tg(ceil_div(L.w, MG_TX), ceil_div(L.h, MG_TY));
+      k_mg_rb2<TM, true><<<tg, 256, mg_rb2_smem<TM, true>(), st>>>(L, C, nullptr);
+      count_launch();
+      TM* zc = vcycle<TM>(s, H, l + 1, kind, st);
+      k_mg_rb2<TM, false><<<tg, 256, mg_rb2_smem<TM, false>(), st>>>(L, C, zc);
+      count_launch();
+      return L.z;
+    }
+  }
   for (int sweep = 0; sweep < NU; ++sweep)
     for (int c = 0; c < ncol; ++c) {
       if (sweep == 0)
@@ -1049,19 +1363,36 @@ static dt_status diff_first_guess(dt_diff* s, const dt_diff_params* p, double dt
       const dim3 tb(32, 8), tg_in(ceil_div(s->w, 32), ceil_div(s->h, 32)), tg_out(ceil_div(s->h, 32), ceil_div(s->w, 32));
       k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->kd, s->lod[0]);
       k_transpose<<<tg_in, tb, 0, st>>>(s->h, s->w, s->x, s->lod[1]);
-      // the walks leave x, z and each row's Sherman-Morrison factor (lod[5]); one parallel pass combines them
-      k_lod_rows_wrap_t<<<ceil_div(s->h, 32), 32, 0, st>>>(s->w, s->h, dtdx2, s->lod[0], s->lod[1], s->lod[2], s->lod[3],
-                                                         s->lod[4], s->lod[5]);
-      k_lod_rows_combine<<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, s->lod[3], s->lod[4], s->lod[5], s->lod[1]);
+      // the rows (lines of w unknowns, h of them) in chunks: lod[1] b -> x, lod[2] z, lod[3] q, lod[4] r,
+      // lod[5] c, lod[6] the chunks' end values and the recurrence's scratch (8 + 4 values a chunk)
+      // and the rows' Sherman-Morrison factors
+      const int P = (int)ceil_div(s->w, LOD_CHUNK);
+      double* edge = s->lod[6];
+      double* al = edge + (size_t)8 * P * s->h;
+      double* fact = al + (size_t)4 * P * s->h;
+      k_lod_chunks<true><<<ceil_div((size_t)s->h * P, 128), 128, 0, st>>>(s->h, s->w, P, dtdx2, s->lod[0], s->lod[1], s->lod[2],
+                                                                        s->lod[3], s->lod[4], s->lod[5], edge);
+      k_lod_reduce<true><<<ceil_div(s->h, 128), 128, 0, st>>>(s->h, s->w, P, dtdx2, s->lod[0], edge, al, fact);
+      k_lod_finish<true><<<dgrid(s, s->n), 256, 0, st>>>(s->h, s->w, P, s->lod[1], s->lod[2], s->lod[3], s->lod[4], edge, fact);
       k_transpose<<<tg_out, tb, 0, st>>>(s->w, s->h, s->lod[1], s->x);
-      for (int k = 0; k < 5; ++k) count_launch();
+      for (int k = 0; k < 6; ++k) count_launch();
     } else {
       k_lod_rows<<<ceil_div(s->h, 64), 64, 0, st>>>(s->w, s->h, s->wrap, s->x, s->kd, dtdx2, s->lod[0], s->lod[1], s->lod[2],
                                                     s->lod[3], s->lod[4], s->lod[5]);
       count_launch();
     }
-    k_lod_cols_fast<<<ceil_div(s->w, 32), 32, 0, st>>>(s->w, s->h, s->x, s->kd, dtdx2, s->lod[5]);
-    count_launch();
+    {
+      // the columns (lines of h unknowns, w of them, as they lie) in chunks: x in place, lod[2] q,
+      // lod[3] r, lod[4] c, lod[6] the chunks' end values
+      const int P = (int)ceil_div(s->h, LOD_CHUNK);
+      double* edge = s->lod[6];
+      double* al = edge + (size_t)8 * P * s->w;
+      k_lod_chunks<false><<<ceil_div((size_t)s->w * P, 128), 128, 0, st>>>(s->w, s->h, P, dtdx2, s->kd, s->x, nullptr,
+                                                                         s->lod[2], s->lod[3], s->lod[4], edge);
+      k_lod_reduce<false><<<ceil_div(s->w, 128), 128, 0, st>>>(s->w, s->h, P, dtdx2, s->kd, edge, al, nullptr);
+      k_lod_finish<false><<<dgrid(s, s->n), 256, 0, st>>>(s->w, s->h, P, s->x, nullptr, s->lod[2], s->lod[3], edge, nullptr);
+      for (int k = 0; k < 3; ++k) count_launch();
+    }
   }
   return DT_OK;
 }
@@ -1083,7 +1414,7 @@ static dt_status solve_fp64_cg(dt_diff* s, const dt_diff_params* p, int lane, dt
   cudaStream_t st = s->stream;
   Hier<TM>& H = hier_for<TM>(s, p->cycle);
   DT_TRY(build_levels<TM>(s, H, p->cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
-  fill_levels<TM>(s, H, st);
+  fill_levels<TM>(s, H, p->cycle, st);
   unsigned int g = dgrid(s, s->n);
   int wrap = s->wrap && s->w > 1;
   // bb, then r = b - A x, rm, rr
@@ -1105,7 +1436,7 @@ static dt_status solve_mixed_cg(dt_diff* s, const dt_diff_params* p, dt_report* 
   cudaStream_t st = s->stream;
   Hier<float>& H = s->hf[p->cycle];
   DT_TRY(build_levels<float>(s, H, p->cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
-  fill_levels<float>(s, H, st);
+  fill_levels<float>(s, H, p->cycle, st);
   unsigned int g = dgrid(s, s->n);
   int wrap = s->wrap && s->w > 1;
   k_d_dot<double><<<g, 256, 0, st>>>(s->n, s->b, s->b, s->partials, s->S64);
@@ -1221,6 +1552,15 @@ dt_status dt_diff_create(int w, int h, double dx, int wrap_x, dt_diff** out) {
   s->h = h;
   s->dx = dx;
   s->wrap = wrap_x ? 1 : 0;
+  if (const char* e = getenv("DT_MG_FUSED")) s->mg_fused = e[0] != '0';
+  // the one-block coarse cycle stages at most about 4/3 MG_BLOCK_CELLS cells (plus the levels'
+  // rounding up) in six arrays
+  cudaFuncSetAttribute(k_mg_coarse_rb<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_mg_coarse_rb<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(k_mg_rb2<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<float, true>());
+  cudaFuncSetAttribute(k_mg_rb2<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<float, false>());
+  cudaFuncSetAttribute(k_mg_rb2<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<double, true>());
+  cudaFuncSetAttribute(k_mg_rb2<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<double, false>());
   s->n = (size_t)w * h;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, 0) == cudaSuccess) s->sms = prop.multiProcessorCount;
@@ -1237,6 +1577,12 @@ dt_status dt_diff_create(int w, int h, double dx, int wrap_x, dt_diff** out) {
     if ((st = ddalloc(s, q, s->n)) != DT_OK) return fail(st);
   for (int k = 0; k < 6; ++k)
     if ((st = ddalloc(s, &s->lod[k], s->n)) != DT_OK) return fail(st);
+  {
+    // the LOD chunks' end values, their recurrence's scratch (12 values a chunk of a line) and
+    // the rows' Sherman-Morrison factors
+    const size_t chunks = (size_t)ceil_div(s->w, LOD_CHUNK) * s->h + (size_t)ceil_div(s->h, LOD_CHUNK) * s->w;
+    if ((st = ddalloc(s, &s->lod[6], 12 * chunks + s->h + s->w)) != DT_OK) return fail(st);
+  }
   if ((st = ddalloc(s, &s->partials, (size_t)s->sms * 8 * 2)) != DT_OK) return fail(st);
   if ((st = ddalloc(s, &s->scale, 1)) != DT_OK) return fail(st);
   if ((st = ddalloc(s, &s->S64, 1)) != DT_OK) return fail(st);
@@ -1423,7 +1769,7 @@ dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, con
                                              s->south32, s->diag32);
   Hier<float>& H = s->hf[cycle];
   DT_TRY(build_levels<float>(s, H, cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
-  fill_levels<float>(s, H, st);
+  fill_levels<float>(s, H, cycle, st);
   k_convert_dr<<<dgrid(s, s->n), 256, 0, st>>>(s->n, s->r, H.lv[0].r);
   float* zz = vcycle<float>(s, H, 0, cycle, st);
   DT_CUDA(cudaGetLastError());

@@ -149,3 +149,30 @@ def test_the_lod_first_guess_matches_the_oracle(wrap):
         got = ws.lod(b, kd, 2.0e6)
         want = O.diff_lod(b, kd, 2.0e6, 2400.0, wrap)
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max(), (w, h, wrap)
+
+
+@pytest.mark.parametrize("w,h,wrap", [(2048, 1024, True), (257, 129, True), (300, 200, False), (96, 48, True), (64, 40, True),
+                                      (41, 9, True)])
+def test_the_fused_gauss_seidel_cycle_is_bit_for_bit_the_per_colour_launches(w, h, wrap, monkeypatch):
+    # the two sweeps of a level in one tiled launch and the levels of <= 2048 cells in one block
+    # (the default) against one launch per colour pass (DT_MG_FUSED=0 at create): the same
+    # updates in the same order, so the same bits for the FP32 cycle
+    z0 = terrain(w, h, 11)
+    kd = shelf_kd(z0, 11)
+    r = np.random.default_rng(w + h).random((h, w)) - 0.5
+    fused = D.Workspace(D.Dims(w, h, 2400.0, wrap))
+    monkeypatch.setenv("DT_MG_FUSED", "0")
+    apart = D.Workspace(D.Dims(w, h, 2400.0, wrap))
+    monkeypatch.delenv("DT_MG_FUSED")
+    for _ in range(2):
+        zf, lf = fused.vcycle(kd, 2.0e6, r, L.CYCLE_RBGS)
+        za, la = apart.vcycle(kd, 2.0e6, r, L.CYCLE_RBGS)
+        assert lf == la and np.array_equal(zf, za), float(np.abs(zf - za).max())
+    # solves: the mixed one's FP32 cycle is bit for bit; in FP64 the compiler forms fused
+    # multiply-adds differently in the two kernels, so the answers agree to 1e-12 relative
+    for precision in (L.DIFF_FP64, L.DIFF_MIXED):
+        p = D.params(cycle=L.CYCLE_RBGS, precision=precision, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000)
+        xf, rf = fused.solve_with(z0, kd, 2.0e6, p)
+        xa, ra = apart.solve_with(z0, kd, 2.0e6, p)
+        assert rf.iterations == ra.iterations, (precision, rf.iterations, ra.iterations)
+        assert np.abs(xf - xa).max() <= 1e-12 * np.abs(xa).max(), (precision, float(np.abs(xf - xa).max()))
