@@ -24,8 +24,8 @@
 //                     each cell's coupling (diffusion.rs:387-500, :283-301).
 //
 // The grid's geometry (neighbour slots, the coupling Laplacian's weights, the cell areas) comes
-// from the caller's CubeGrid at create. The CG loop is driven from the host (three scalars read
-// back an iteration).
+// from the caller's CubeGrid at create. The CG loop runs on the device as a CUDA graph (a WHILE
+// node, the iteration's tail under an IF node), with one read back at its end.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -144,10 +144,16 @@ __global__ void k_cube_dot(size_t cells, const double* __restrict__ a, const dou
 }
 
 // the direction pn = z + beta po (z alone on the first), A pn, partial pn.A pn (diffusion.rs:407-443)
+// loop: the device loop's scalars (null when the host drives the loop): its stop flag ends the
+// kernel's work, its iteration count tells the first direction
 __global__ void k_cube_direction(size_t cells, const uint32_t* __restrict__ slots, const double* __restrict__ k,
                                  const double* __restrict__ diag, const double* __restrict__ z, const double* __restrict__ po,
                                  const double* __restrict__ beta_p, int first, double* __restrict__ pn,
-                                 double* __restrict__ ap, double* __restrict__ partials) {
+                                 double* __restrict__ ap, double* __restrict__ partials, const double* __restrict__ loop) {
+  if (loop) {
+    if (loop[13] != 0.0) return;
+    first = loop[12] == 0.0;
+  }
   const double beta = first ? 0.0 : *beta_p;
   auto dir = [&](size_t j) { return first ? z[j] : __dadd_rn(z[j], __dmul_rn(beta, po[j])); };
   double acc = 0.0;
@@ -165,8 +171,9 @@ __global__ void k_cube_direction(size_t cells, const uint32_t* __restrict__ slot
 // x += alpha p; r -= alpha A p; partial r.r (diffusion.rs:448-475)
 __global__ void k_cube_update(size_t cells, const double* __restrict__ alpha_p, const double* __restrict__ broke,
                               const double* __restrict__ p, const double* __restrict__ ap, double* __restrict__ x,
-                              double* __restrict__ r, double* __restrict__ partials) {
+                              double* __restrict__ r, double* __restrict__ partials, const double* __restrict__ loop) {
   if (*broke != 0.0) return;  // the loop stops before the update
+  if (loop && loop[13] != 0.0) return;
   const double alpha = *alpha_p;
   double acc = 0.0;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) {
@@ -449,7 +456,8 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_cycle(MgCoarse m) {
 // alpha = rz / pap; beta = rz_new / rz, rz = rz_new (the CG scalars, on the device)
 // alpha = rz / pap, or the breakdown flag (pap not positive, or NaN: diffusion.rs:444-446)
 __global__ void k_cube_alpha(const double* __restrict__ rz, const double* __restrict__ pap, double* __restrict__ alpha,
-                             double* __restrict__ broke) {
+                             double* __restrict__ broke, const double* __restrict__ loop) {
+  if (loop && loop[13] != 0.0) return;
   const double p = *pap;
   if (isnan(p) || p <= 0.0) {
     *broke = 1.0;
@@ -461,6 +469,32 @@ __global__ void k_cube_alpha(const double* __restrict__ rz, const double* __rest
 __global__ void k_cube_beta(const double* __restrict__ rz_new, double* __restrict__ rz, double* __restrict__ beta) {
   *beta = *rz_new / *rz;
   *rz = *rz_new;
+}
+
+// The device loop's control: sc[12] iterations, sc[13] the stop flag, sc[14] tol^2 n, sc[15] the
+// iteration cap. After an iteration's update (or its breakdown): the host loop's tests, the
+// WHILE node's condition and the IF node's around the iteration's tail (preconditioner, r.z,
+// beta), so that nothing runs after the stop.
+__global__ void k_cube_arm(const double* __restrict__ sc, unsigned long long while_h) {
+  cudaGraphSetConditional((cudaGraphConditionalHandle)while_h, sc[13] == 0.0 ? 1u : 0u);
+}
+__global__ void k_cube_check(double* __restrict__ sc, unsigned long long while_h, unsigned long long if_h) {
+  bool stop = sc[13] != 0.0;
+  if (!stop) {
+    if (sc[10] != 0.0) {  // p.Ap not positive or NaN: no update (diffusion.rs:444-446)
+      stop = true;
+    } else {
+      sc[0] = sc[11];
+      sc[12] += 1.0;
+      stop = sc[11] <= sc[14] || sc[12] >= sc[15];
+    }
+  }
+  if (stop) sc[13] = 1.0;
+  cudaGraphSetConditional((cudaGraphConditionalHandle)while_h, stop ? 0u : 1u);
+  cudaGraphSetConditional((cudaGraphConditionalHandle)if_h, stop ? 0u : 1u);
+}
+__global__ void k_cube_copy(size_t cells, const double* __restrict__ a, double* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cells; i += (size_t)gridDim.x * blockDim.x) b[i] = a[i];
 }
 
 // partials of (rhs - ap) and of s, for the put-back
@@ -584,6 +618,12 @@ struct dt_cube {
   // first use.
   cudaGraphExec_t vcycle_exec[2] = {nullptr, nullptr};
   int vcycle_layout = 0;
+  // the CG loop as a graph (a WHILE node over one iteration, the tail under an IF node), made on
+  // the first solve; DT_CUBE_HOST_LOOP=1 at create drives the loop from the host instead (the
+  // same kernels, three scalars read back an iteration)
+  cudaGraphExec_t cg_exec = nullptr;
+  cudaStream_t aside = nullptr;
+  bool host_loop = false;
   // levels of at most this many cells run their part of the cycle in one block; the environment
   // variable DT_CUBE_FUSE_CELLS, read at dt_cube_create, overrides it (0: every level launches
   // its own kernels, the form the fused block reproduces bit for bit)
@@ -743,6 +783,105 @@ double read_scalar(dt_cube* s, int i) {
   return v;
 }
 
+// The CG loop as a graph, made once per handle: arm -> WHILE { direction + A p + p.Ap, alpha, x and
+// r with r.r, the stop test; IF not stopped { p_old = p, the V-cycle, r.z, beta } }. The same
+// kernels and values as the host-driven loop; the buffers are fixed, so the new direction is
+// copied to p_old where the host loop swaps the two.
+dt_status cube_cg_graph(dt_cube* s) {
+  if (s->cg_exec) return DT_OK;
+  if (!s->aside) DT_CUDA(cudaStreamCreateWithFlags(&s->aside, cudaStreamNonBlocking));
+  const size_t l = s->cells;
+  const unsigned int G = CUBE_RED_BLOCKS;
+  cudaGraph_t g = nullptr;
+  DT_CUDA(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hw;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+  unsigned long long hwv = (unsigned long long)hw;
+  double* sc = s->sc;
+  void* arm_args[] = {&sc, &hwv};
+  cudaKernelNodeParams kp = {};
+  kp.func = (void*)k_cube_arm;
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(1);
+  kp.kernelParams = arm_args;
+  cudaGraphNode_t n_arm, n_loop;
+  DT_CUDA(cudaGraphAddKernelNode(&n_arm, g, nullptr, 0, &kp));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = hw;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphConditionalHandle hif;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&hif, body, 0, cudaGraphCondAssignDefault));
+  const unsigned long long hifv = (unsigned long long)hif;
+  if (cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    set_error("dt_cube: the CG loop's graph: the stream cannot be captured");
+    return DT_DEVICE_ERROR;
+  }
+  k_cube_direction<<<G, 256, 0, s->stream>>>(l, s->slots, s->k, s->diag, s->z, s->po, s->sc + 5, 0, s->pn, s->ap, s->partials,
+                                             s->sc);
+  cube_finish(s, s->partials, s->sc + 1);
+  k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4, s->sc + 10, s->sc);
+  k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->sc + 10, s->pn, s->ap, s->x, s->r, s->partials, s->sc);
+  cube_finish(s, s->partials, s->sc + 11);
+  k_cube_check<<<1, 1, 0, s->stream>>>(s->sc, hwv, hifv);
+  // the IF node after the head, its body captured on the side stream (the launch helpers use
+  // s->stream, so it stands in for the side stream meanwhile; the capture's host-side swaps of
+  // the levels' sweep buffers are undone after it)
+  cudaError_t err = cudaSuccess;
+  {
+    cudaStreamCaptureStatus csx;
+    unsigned long long id = 0;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    err = cudaStreamGetCaptureInfo(s->stream, &csx, &id, &cg, &deps, &nd);
+    cudaGraphNodeParams ip = {};
+    ip.type = cudaGraphNodeTypeConditional;
+    ip.conditional.handle = hif;
+    ip.conditional.type = cudaGraphCondTypeIf;
+    ip.conditional.size = 1;
+    cudaGraphNode_t n_if;
+    if (err == cudaSuccess) err = cudaGraphAddNode(&n_if, cg, deps, nd, &ip);
+    if (err == cudaSuccess) err = cudaStreamUpdateCaptureDependencies(s->stream, &n_if, 1, cudaStreamSetCaptureDependencies);
+    if (err == cudaSuccess)
+      err = cudaStreamBeginCaptureToGraph(s->aside, ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                          cudaStreamCaptureModeThreadLocal);
+    if (err == cudaSuccess) {
+      std::vector<std::pair<float*, float*>> keep;
+      for (const CubeLevel& lv : s->levels) keep.emplace_back(lv.z, lv.t);
+      cudaStream_t main = s->stream;
+      s->stream = s->aside;
+      k_cube_copy<<<cube_grid(l), 256, 0, s->stream>>>(l, s->pn, s->po);
+      cube_precondition_launches(s, s->r, s->z);
+      k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
+      cube_finish(s, s->partials, s->sc + 3);
+      k_cube_beta<<<1, 1, 0, s->stream>>>(s->sc + 3, s->sc + 2, s->sc + 5);
+      s->stream = main;
+      for (size_t q = 0; q < s->levels.size(); ++q) {
+        s->levels[q].z = keep[q].first;
+        s->levels[q].t = keep[q].second;
+      }
+      cudaGraph_t ifbody = nullptr;
+      err = cudaStreamEndCapture(s->aside, &ifbody);
+    }
+  }
+  cudaGraph_t captured = nullptr;
+  const cudaError_t end = cudaStreamEndCapture(s->stream, &captured);
+  if (err == cudaSuccess) err = end;
+  if (err == cudaSuccess) err = cudaGraphInstantiate(&s->cg_exec, g, 0);
+  cudaGraphDestroy(g);
+  if (err != cudaSuccess) {
+    s->cg_exec = nullptr;
+    set_error("dt_cube: the CG loop's graph: %s", cudaGetErrorString(err));
+    return DT_DEVICE_ERROR;
+  }
+  return DT_OK;
+}
+
 // The solve's two timing events, destroyed on every way out.
 struct EventPair {
   cudaEvent_t a = nullptr, b = nullptr;
@@ -780,13 +919,33 @@ dt_status cube_solve(dt_cube* s, double* h, const double* kd, double dt, double 
     DT_TRY(cube_precondition(s));
     k_cube_dot<<<G, 256, 0, s->stream>>>(l, s->r, s->z, s->partials);
     cube_finish(s, s->partials, s->sc + 2);
-    for (int it = 0; it < CUBE_CG_MAX_ITER; ++it) {
+    // the loop on the device, one read back at its end; on a stream that cannot be captured (the
+    // legacy default stream), driven from the host
+    bool host = s->host_loop;
+    if (!host && cube_cg_graph(s) != DT_OK) {
+      cudaGetLastError();
+      host = true;
+    }
+    if (!host) {
+      const double init[4] = {0.0, 0.0, tol2, (double)CUBE_CG_MAX_ITER};
+      DT_CUDA(cudaMemcpyAsync(s->sc + 12, init, sizeof init, cudaMemcpyHostToDevice, s->stream));
+      DT_CUDA(cudaGraphLaunch(s->cg_exec, s->stream));
+      double back[13];
+      if (cudaMemcpyAsync(back, s->sc, sizeof back, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+          cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        back[0] = std::nan("");
+        back[12] = 0.0;
+      }
+      rr = back[0];
+      iterations = (int)back[12];
+    }
+    for (int it = 0; host && it < CUBE_CG_MAX_ITER; ++it) {
       k_cube_direction<<<G, 256, 0, s->stream>>>(l, s->slots, s->k, s->diag, s->z, s->po, s->sc + 5, it == 0, s->pn, s->ap,
-                                                 s->partials);
+                                                 s->partials, nullptr);
       cube_finish(s, s->partials, s->sc + 1);
       std::swap(s->po, s->pn);
-      k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4, s->sc + 10);
-      k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->sc + 10, s->po, s->ap, s->x, s->r, s->partials);
+      k_cube_alpha<<<1, 1, 0, s->stream>>>(s->sc + 2, s->sc + 1, s->sc + 4, s->sc + 10, nullptr);
+      k_cube_update<<<G, 256, 0, s->stream>>>(l, s->sc + 4, s->sc + 10, s->po, s->ap, s->x, s->r, s->partials, nullptr);
       cube_finish(s, s->partials, s->sc + 11);
       // one read back an iteration: the new r.r and the breakdown flag
       double back[2] = {std::nan(""), 1.0};
@@ -847,6 +1006,8 @@ dt_status dt_cube_destroy(dt_cube* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (cudaGraphExec_t& e : s->vcycle_exec)
     if (e) cudaGraphExecDestroy(e);
+  if (s->cg_exec) cudaGraphExecDestroy(s->cg_exec);
+  if (s->aside) cudaStreamDestroy(s->aside);
   for (void* p : s->allocs) cudaFree(p);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
@@ -886,6 +1047,7 @@ dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const 
   s->n = n;
   s->fuse_cells = CUBE_FUSE_CELLS;
   if (const char* e = std::getenv("DT_CUBE_FUSE_CELLS")) s->fuse_cells = std::strtoull(e, nullptr, 10);
+  if (const char* e = std::getenv("DT_CUBE_HOST_LOOP")) s->host_loop = e[0] == '1';
   s->cells = cells;
   auto fail = [&](dt_status e) {
     dt_cube_destroy(s);

@@ -588,13 +588,15 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_rb(MgChain<TM> g, int nu, in
 //         tile and its 2 x 2 sums into the coarser level's r (k_mg_restrict's arithmetic), so
 //         the restriction needs no launch of its own (halo 5: z is final one ring out);
 //   !PRE  the post-smoothing: z += P zc (the coarse correction, piecewise constant), then
-//         colours 1, 0, 1, 0 (halo 4).
+//         colours 1, 0, 1, 0 (halo 4). It reads z around its tile, which neighbouring tiles
+//         finish at the same time, so it writes its result to another buffer (zout = L.t; PRE,
+//         which reads no z, writes L.z).
 // For levels of two colours (no wrap, or an even width) at least MG_TX + 10 cells wide, so that
 // no cell sits twice in a tile. Shared memory holds the region in red-black order, so that a
 // colour pass reads and writes consecutive words with no idle lanes.
 constexpr int MG_TX = 32, MG_TY = 16;
 template <class TM, bool PRE>
-__global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, const TM* __restrict__ zc) {
+__global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, const TM* __restrict__ zc, TM* __restrict__ zout) {
   constexpr int HALO = PRE ? 5 : 4;
   constexpr int SX = MG_TX + 2 * HALO, SY = MG_TY + 2 * HALO;
   constexpr int HX = SX / 2, NC = HX * SY;  // a colour's cells of a row, of the region
@@ -690,7 +692,7 @@ __global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, cons
   for (int e = tid; e < MG_TX * MG_TY; e += 256) {
     const int ly = HALO + e / MG_TX, lx = HALO + e % MG_TX;
     const int gi = i0 + lx, gj = j0 + ly;
-    if (gi < w && gj < h) L.z[(size_t)gj * w + gi] = at(0, lx, ly);
+    if (gi < w && gj < h) zout[(size_t)gj * w + gi] = at(0, lx, ly);
   }
 }
 template <class TM, bool PRE>
@@ -1215,12 +1217,12 @@ static TM* vcycle(dt_diff* s, Hier<TM>& H, size_t l, int kind, cudaStream_t st) 
     // pre-smoothing (two-colour levels wide enough)
     if (ncol == 2 && NU == 2 && L.w >= MG_TX + 10) {
       const dim3 tg(ceil_div(L.w, MG_TX), ceil_div(L.h, MG_TY));
-      k_mg_rb2<TM, true><<<tg, 256, mg_rb2_smem<TM, true>(), st>>>(L, C, nullptr);
+      k_mg_rb2<TM, true><<<tg, 256, mg_rb2_smem<TM, true>(), st>>>(L, C, nullptr, L.z);
       count_launch();
       TM* zc = vcycle<TM>(s, H, l + 1, kind, st);
-      k_mg_rb2<TM, false><<<tg, 256, mg_rb2_smem<TM, false>(), st>>>(L, C, zc);
+      k_mg_rb2<TM, false><<<tg, 256, mg_rb2_smem<TM, false>(), st>>>(L, C, zc, L.t);
       count_launch();
-      return L.z;
+      return L.t;  // the level's z, in its spare buffer
     }
   }
   for (int sweep = 0; sweep < NU; ++sweep)

@@ -101,3 +101,21 @@ def test_the_one_block_coarse_cycle_is_bit_for_bit_the_separate_launches(n, monk
     xa, ra = fused.solve(h, kd, 7.0, 1e-6)
     xb, rb = apart.solve(h, kd, 7.0, 1e-6)
     assert ra.iterations == rb.iterations and np.array_equal(xa, xb)
+
+
+@pytest.mark.parametrize("n", [13, 64])
+def test_the_device_loop_is_bit_for_bit_the_host_driven_one(n, monkeypatch):
+    """The CG loop as a CUDA graph (the default: a WHILE node, the iteration's tail under an IF
+    node) against the loop driven from the host (DT_CUBE_HOST_LOOP=1 at create): the same kernels
+    in the same order, so the same iterations and the same bits, twice in a row on each handle."""
+    slots = O.cube_topology(n)
+    lap, areas, kd, h = cube_case(n, n + 300, slots)
+    graph = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.setenv("DT_CUBE_HOST_LOOP", "1")
+    host = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.delenv("DT_CUBE_HOST_LOOP")
+    for dt in (7.0, 60.0, 7.0):
+        xg, rg = graph.solve(h, kd, dt, 1e-6)
+        xh, rh = host.solve(h, kd, dt, 1e-6)
+        assert rg.iterations == rh.iterations and rg.converged == rh.converged
+        assert np.array_equal(xg, xh), float(np.abs(xg - xh).max())
