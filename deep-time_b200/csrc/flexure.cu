@@ -1667,6 +1667,149 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   }
 }
 
+// k_rows_inv's INV_BANK (one row a block) as a persistent kernel fed by bulk copies: block b
+// takes rows b, b + gridDim.x, ..., each row's three levels in turn. A level's half row (N complex
+// values) and weight row (2 N) land in shared memory by two 1-D bulk copies on two mbarriers; the
+// next level's half row is copied as soon as this level's split has read it, its weight row as
+// soon as this level's sums have read theirs, so both copies overlap the transform. The three
+// levels' weighted outputs are summed in registers and stored once a row. Arithmetic and order of
+// operations are k_rows_inv's. Waits are bounded: one that runs out flags a fault, stops the
+// solve and waits (bounded again) for the copies in flight before the block leaves.
+template <class T>
+__host__ __device__ constexpr size_t rows_bank_smem(int logn) {
+  return ((size_t)1 << logn) * 2 * sizeof(T) * 2 + (size_t)Pad<cplx<T>>::len(1 << logn) * 2 * sizeof(T);
+}
+template <class T, int LOGN>
+__global__ void __launch_bounds__((1 << LOGN) / FFT_EPT, (1 << LOGN) / FFT_EPT <= 128 && sizeof(T) == 4 ? 4 : 2)
+    k_rows_inv_bank(int h, const cplx<T>* __restrict__ half, T* __restrict__ out, const T* __restrict__ wt,
+                    const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ post, Scalars* S) {
+  using C = cplx<T>;
+  using P = Pad<C>;
+  if (S->stop) return;
+  constexpr int N = 1 << LOGN;
+  constexpr int NT = N / FFT_EPT;
+  constexpr int RL = last_radix(LOGN);
+  constexpr int LOGRL = RL == 16 ? 4 : RL == 8 ? 3 : RL == 4 ? 2 : 1;
+  constexpr int NSL = N / RL;
+  constexpr int Q = FFT_EPT / RL;
+  constexpr uint32_t XB = N * sizeof(C), WB = 2 * N * sizeof(T);
+  static_assert(LOGN >= 4 && NSL % 16 == 0, "one row a block");
+  extern __shared__ __align__(128) unsigned char rb_smem[];
+  C* xs = reinterpret_cast<C*>(rb_smem);             // the level's half row, as copied
+  const C* ws = reinterpret_cast<const C*>(rb_smem + XB);  // its weight row, as pairs
+  C* s = reinterpret_cast<C*>(rb_smem + XB + WB);    // the transform
+  __shared__ __align__(8) uint64_t bar[2];           // 0: half rows, 1: weight rows
+  __shared__ int s_fail;
+  const int tid = threadIdx.x;
+  const int b0 = blockIdx.x, G = gridDim.x;
+  const int items = b0 < h ? 3 * ((h - 1 - b0) / G + 1) : 0;  // (row, level) pairs, level fastest
+  auto src_off = [&](int i) { return (size_t)(i % 3) * h + (size_t)(b0 + (i / 3) * G); };  // level-major row index
+  auto issue_x = [&](int i) {
+    mbar_expect_tx(smem_u32(&bar[0]), XB);
+    bulk_load_1d(smem_u32(xs), half + src_off(i) * N, XB, smem_u32(&bar[0]));
+  };
+  auto issue_w = [&](int i) {
+    mbar_expect_tx(smem_u32(&bar[1]), WB);
+    bulk_load_1d(smem_u32(rb_smem + XB), wt + src_off(i) * (2 * N), WB, smem_u32(&bar[1]));
+  };
+  if (tid == 0) {
+    mbar_init(smem_u32(&bar[0]), 1);
+    mbar_init(smem_u32(&bar[1]), 1);
+    mbar_fence_init();
+    s_fail = 0;
+    if (items > 0) {
+      issue_x(0);
+      issue_w(0);
+    }
+  }
+  __syncthreads();
+  const int polls = S->wait_give_up ? 0 : 1 << 24;
+  // a wait that ran out: the copies in flight (x_par / w_par: their phases, -1 for none) land
+  // before the block leaves
+  auto fail = [&](int x_par, int w_par) {
+    if (tid == 0) {
+      S->fault = 1;
+      S->stop = STOP_NONFINITE;
+      set_cond(S, 0);
+      if (x_par >= 0) mbar_wait_bounded(smem_u32(&bar[0]), (uint32_t)x_par);
+      if (w_par >= 0) mbar_wait_bounded(smem_u32(&bar[1]), (uint32_t)w_par);
+    }
+  };
+  const T inv_n = (T)1 / (T)N;
+  C acc[Q][RL];
+#pragma unroll 1
+  for (int i = 0; i < items; ++i) {
+    const int lv = i % 3;
+    const uint32_t par = (uint32_t)(i & 1);
+    if (tid == 0 && !mbar_wait_bounded(smem_u32(&bar[0]), par, polls)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      fail((int)par, (int)par);
+      return;
+    }
+    // the split of k_rows_inv: Z[k] = E[k] + i O[k] from the copied half row
+#pragma unroll 2
+    for (int kk = tid; kk < N / 2 + 1; kk += NT) {
+      if (kk == 0) {
+        C p = xs[0];  // (X[0], X[N])
+        s[0] = mk<C>((p.x + p.y) * (T)0.5, (p.x - p.y) * (T)0.5);
+        continue;
+      }
+      C xk = xs[kk], xn = xs[N - kk];
+      C E = mk<C>((xk.x + xn.x) * (T)0.5, (xk.y - xn.y) * (T)0.5);
+      C D = mk<C>((xk.x - xn.x) * (T)0.5, (xk.y + xn.y) * (T)0.5);
+      C pk = post[kk];
+      C O = cmul(D, cconj(pk));
+      s[P::at(kk)] = cadd(E, cmuli(O));
+      if (kk != N - kk) {
+        C O2 = cmul(cconj(D), pk);
+        s[P::at(N - kk)] = cadd(cconj(E), cmuli(O2));
+      }
+    }
+    fence_proxy_async_smem();  // this thread's reads of xs before the next copy into it
+    __syncthreads();
+    if (tid == 0 && i + 1 < items) issue_x(i + 1);
+    Stages<C, FFT_EPT, true, LOGN, 1, LOGN - LOGRL, 0, NT>::run(s, tw);
+    if (tid == 0 && !mbar_wait_bounded(smem_u32(&bar[1]), par, polls)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) {
+      fail(i + 1 < items ? (int)(par ^ 1u) : -1, (int)par);
+      return;
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      const int j = tid + q * NT;
+      C z[RL];
+#pragma unroll
+      for (int rr = 0; rr < RL; ++rr) z[rr] = s[P::at(j) + rr * (NSL + NSL / 16)];
+      C wv[RL];
+      stage_twiddles<C, RL, true>(tw, j, wv);
+#pragma unroll
+      for (int rr = 1; rr < RL; ++rr) z[rr] = cmul(z[rr], wv[rr]);
+      dft_r<C, RL, true>(z);
+#pragma unroll
+      for (int rr = 0; rr < RL; ++rr) {
+        const C zz = cscale(z[rr], inv_n), ww = ws[j + rr * NSL];
+        if (lv == 0) {
+          acc[q][rr] = mk<C>(zz.x * ww.x, zz.y * ww.y);
+        } else {
+          acc[q][rr] = mk<C>(acc[q][rr].x + zz.x * ww.x, acc[q][rr].y + zz.y * ww.y);
+        }
+      }
+    }
+    if (lv == 2) {
+      C* o = reinterpret_cast<C*>(out + (size_t)(b0 + (i / 3) * G) * (2 * N));
+#pragma unroll
+      for (int q = 0; q < Q; ++q)
+#pragma unroll
+        for (int rr = 0; rr < RL; ++rr) o[tid + q * NT + rr * NSL] = acc[q][rr];
+    }
+    fence_proxy_async_smem();  // the reads of ws (and s) before the next copy and split
+    __syncthreads();
+    if (tid == 0 && i + 1 < items) issue_w(i + 1);
+  }
+}
+
 #include "rows_any.cuh"
 
 // ---------------------------------------------------------------------------------------------
@@ -1829,6 +1972,7 @@ struct Lane {
   // the bank's levels 1 and 2 transform beside level 0, into their own spectra: the three
   // spectra are consecutive (half + k h N), as are the three weights (wt[k] = wt[0] + k n)
   cplx<T>* half_side[2] = {nullptr, nullptr};
+  int bank_blocks = 0;  // k_rows_inv_bank's persistent grid (0: not yet known)
   // the row metric's L D L^T factors per bank level: dd, l1, l2 (h x (N + 1) each); when the
   // rows make more than one chunk, per level the chunks' carry transfers (8 x chunks x (N + 1))
   // and the chunk states and carries (4 complex x chunks x (N + 1))
@@ -1882,6 +2026,9 @@ struct dt_flex {
   // the column pass with its divide in registers (k_cols_fused) where the length allows;
   // DT_COLS_FUSED=0 at create keeps k_cols everywhere (the same values, for comparison)
   bool cols_fused = true;
+  // the bank's inverse row pass as the persistent, bulk-copy-fed k_rows_inv_bank where the row
+  // length allows; DT_ROWS_BANK=0 at create keeps k_rows_inv (the same values, for comparison)
+  bool rows_bank = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
@@ -2316,6 +2463,22 @@ static RowsInvFn<T> rows_inv_fn(int logn, std::integer_sequence<int, L...>) {
 }
 using LogSeq = std::make_integer_sequence<int, FFT_LOGS>;
 template <class T>
+using RowsBankFn = void (*)(int, const cplx<T>*, T*, const T*, const cplx<T>*, const cplx<T>*, Scalars*);
+// k_rows_inv_bank for rows of one block (N >= 512) whose three staging buffers take at most
+// 112 KB of shared memory (two blocks an SM at least); null for the others
+template <class T, int L>
+static constexpr RowsBankFn<T> rows_bank_kernel() {
+  if constexpr (L >= 9 && rows_bank_smem<T>(L) <= 112 * 1024)
+    return &k_rows_inv_bank<T, L>;
+  else
+    return nullptr;
+}
+template <class T, int... L>
+static RowsBankFn<T> rows_bank_fn(int logn, std::integer_sequence<int, L...>) {
+  static const RowsBankFn<T> table[] = {rows_bank_kernel<T, L>()...};
+  return table[logn];
+}
+template <class T>
 static RowsInvFn<T> rows_inv_for(int mode, int logn) {
   switch (mode) {
     case INV_STORE: return rows_inv_fn<T, INV_STORE>(logn, LogSeq{});
@@ -2336,6 +2499,8 @@ static void transform_smem_attributes() {
     cudaFuncSetAttribute(cols_fn<T>(l, LogSeq{}, true), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
     for (int m : {INV_STORE, INV_STORE_W, INV_STORE_DOT, INV_BANK})
       cudaFuncSetAttribute(rows_inv_for<T>(m, l), cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+    if (RowsBankFn<T> f = rows_bank_fn<T>(l, LogSeq{}))
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rows_bank_smem<T>(l));
   }
 }
 
@@ -2484,8 +2649,24 @@ static void launch_rows_inv(dt_flex* s, Lane<T>& L, int mode, const cplx<T>* hal
     any_rows_inv<T>(s, L, mode, half, out, wt, r, S, st);
     return;
   }
-  rows_inv_for<T>(mode, ilog2(s->N))<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, half, out, wt, r, L.tab.tw_row,
-                                                                           L.tab.post, s->partials, S);
+  const int logn = ilog2(s->N);
+  if (mode == INV_BANK && s->rows_bank) {
+    if (RowsBankFn<T> f = rows_bank_fn<T>(logn, LogSeq{})) {
+      // persistent: as many blocks as the SMs hold at once, at most one a row
+      const int nt = s->N / FFT_EPT;
+      const size_t smem = rows_bank_smem<T>(logn);
+      if (L.bank_blocks == 0) {
+        int per = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, f, nt, smem) != cudaSuccess || per < 1) per = 1;
+        L.bank_blocks = per * s->sms;
+      }
+      f<<<std::min(s->h, L.bank_blocks), nt, smem, st>>>(s->h, half, out, wt, L.tab.tw_row, L.tab.post, S);
+      counted();
+      return;
+    }
+  }
+  rows_inv_for<T>(mode, logn)<<<g.rgrid, g.rthreads, g.rsmem, st>>>(s->w, s->h, half, out, wt, r, L.tab.tw_row,
+                                                                    L.tab.post, s->partials, S);
   counted();
 }
 
@@ -3158,6 +3339,7 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   s->own_stream = true;
   if (const char* e = getenv("DT_STENCIL_WAIT_GIVE_UP")) s->wait_give_up = e[0] == '1';
   if (const char* e = getenv("DT_COLS_FUSED")) s->cols_fused = e[0] != '0';
+  if (const char* e = getenv("DT_ROWS_BANK")) s->rows_bank = e[0] != '0';
 
   // RowMetric::block (flexure.rs:1000-1010): the block metric's couplings, for a height the
   // cosine transform does not take

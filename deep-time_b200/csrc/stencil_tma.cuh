@@ -57,6 +57,13 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(mbar)
       : "memory");
 }
+// A contiguous copy of `bytes` (a multiple of 16; both addresses 16-byte aligned) from global
+// memory into this CTA's shared memory, completing on the mbarrier.
+__device__ __forceinline__ void bulk_load_1d(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(reinterpret_cast<unsigned long long>(src)), "r"(bytes), "r"(mbar)
+               : "memory");
+}
 // Orders this thread's generic-proxy shared-memory accesses before later async-proxy (TMA) ones.
 __device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
