@@ -735,6 +735,7 @@ def diffusion_leg(lib, stream, timed, max_over_ranks, world, steps, check=True):
     out = {"workload": f"implicit diffusion {w}x{h}, kappa dt/dx^2 log-uniform [0.1, 100], CG to rel. residual 1e-10"}
     answers = {}
     for name, cycle, prec in (("fp64_rbgs", L.CYCLE_RBGS, L.DIFF_FP64), ("mixed_rbgs", L.CYCLE_RBGS, L.DIFF_MIXED),
+                              ("mixed_reliable_rbgs", L.CYCLE_RBGS, L.DIFF_MIXED_RELIABLE),
                               ("reference_split_jacobi", L.CYCLE_JACOBI, L.DIFF_FP64_CG_FP32_CYCLE)):
         p = D.params(cycle=cycle, precision=prec, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000)
         solve(0, p)
@@ -757,6 +758,7 @@ def diffusion_leg(lib, stream, timed, max_over_ranks, world, steps, check=True):
             out[name]["rel_l2"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
             out[name]["max_abs_m"] = float(np.abs(got - exact).max())
     out["speedup_mixed_vs_fp64"] = out["fp64_rbgs"]["ms_per_solve"] / out["mixed_rbgs"]["ms_per_solve"]
+    out["speedup_mixed_reliable_vs_fp64"] = out["fp64_rbgs"]["ms_per_solve"] / out["mixed_reliable_rbgs"]["ms_per_solve"]
     ws.close()
     return out
 

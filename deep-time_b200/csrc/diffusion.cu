@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -45,6 +46,12 @@ struct DScalars {
   double lost, weight, dot_out;
   unsigned long long cond;
   unsigned int ticket[8];
+  // reliable updates (DT_DIFF_MIXED_RELIABLE, the FP32 lane): the FP32 residual is replaced by
+  // the FP64 one, and x folded into the FP64 accumulation, whenever rr has fallen below
+  // delta2 * maxrr or under the tolerance; gate_it == it marks an iteration that does so
+  int reliable, gate_it, replacements;
+  double delta2, maxrr, rr_true, bb_true;  // rr_true, bb_true: ||b - A x||^2, the reference ||b||^2, unscaled
+  unsigned long long cond_if;              // the loop body's IF node around the replacement, 0 without one
 };
 
 __device__ __forceinline__ void dset_cond(DScalars* S, unsigned int v) {
@@ -105,10 +112,11 @@ __device__ __forceinline__ T d_apply_at(int w, int h, bool wrap, const T* __rest
   return o;
 }
 
-enum { DA_PAP = 0, DA_RESID = 1, DA_MASS = 2, DA_PLAIN = 3 };
+enum { DA_PAP = 0, DA_RESID = 1, DA_MASS = 2, DA_PLAIN = 3, DA_RESID_GATED = 4 };
 
 // DA_PAP: y = A x, reduce x.y; DA_RESID: y = b - A x, ym = (TM) y, reduce y.y;
-// DA_MASS: reduce sum (b - A x) and sum (diag - 1); DA_PLAIN: y = A x.
+// DA_MASS: reduce sum (b - A x) and sum (diag - 1); DA_PLAIN: y = A x; DA_RESID_GATED: in an
+// iteration that replaces the residual (S->gate_it == S->it), y = b - A x and y.y -> S->rr_true.
 template <class T, class TM, int MODE>
 __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T* __restrict__ east, const T* __restrict__ south,
                                                  const T* __restrict__ diag, const T* __restrict__ x, const T* __restrict__ b,
@@ -117,6 +125,7 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
     if (blockIdx.x == 0 && threadIdx.x == 0) dset_cond(S, 0);
     return;
   }
+  if (MODE == DA_RESID_GATED && (S->stop || S->gate_it != S->it)) return;
   size_t n = (size_t)w * h;
   Acc<2> acc;
   acc.v[0] = 0.0;
@@ -132,6 +141,10 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
       y[k] = r;
       ym[k] = (TM)r;
       acc.v[0] += (double)r * (double)r;
+    } else if (MODE == DA_RESID_GATED) {
+      T r = b[k] - ax;
+      y[k] = r;
+      acc.v[0] += (double)r * (double)r;
     } else if (MODE == DA_MASS) {
       acc.v[0] += (double)b[k] - (double)ax;
       acc.v[1] += (double)diag[k] - 1.0;
@@ -141,7 +154,7 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
   }
   if (MODE == DA_PLAIN) return;
   const int kind[2] = {0, 0};
-  int site = MODE == DA_PAP ? DSITE_PAP : MODE == DA_RESID ? DSITE_RESID : DSITE_MASS;
+  int site = MODE == DA_PAP ? DSITE_PAP : (MODE == DA_RESID || MODE == DA_RESID_GATED) ? DSITE_RESID : DSITE_MASS;
   if (reduce_partials<2>(acc, kind, partials, &S->ticket[site], gridDim.x) && threadIdx.x == 0) {
     if (MODE == DA_PAP) {
       S->pap = acc.v[0];
@@ -153,6 +166,8 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
       }
     } else if (MODE == DA_RESID) {
       S->rr = acc.v[0];
+    } else if (MODE == DA_RESID_GATED) {
+      S->rr_true = acc.v[0];
     } else {
       S->lost = acc.v[0];
       S->weight = acc.v[1];
@@ -183,6 +198,21 @@ __global__ void __launch_bounds__(256) k_d_update(size_t n, T* __restrict__ x, T
     double rr = acc.v[0];
     S->rr = rr;
     S->it += 1;
+    if (S->reliable) {
+      // the FP32 residual only asks for a replacement; the FP64 residual decides convergence
+      bool gate = false;
+      if (!isfinite(rr)) {
+        S->stop = DSTOP_NONFINITE;
+      } else if (rr <= S->tol * S->tol * S->bb || rr < S->delta2 * S->maxrr) {
+        S->gate_it = S->it;
+        gate = true;
+      } else if (S->it >= S->max_it) {
+        S->stop = DSTOP_CAP;
+      }
+      if (S->cond_if) cudaGraphSetConditional((cudaGraphConditionalHandle)S->cond_if, gate ? 1u : 0u);
+      if (S->stop) dset_cond(S, 0);
+      return;
+    }
     if (!isfinite(rr))
       S->stop = DSTOP_NONFINITE;
     else if (d_converged(S, rr))
@@ -966,16 +996,21 @@ __global__ void __launch_bounds__(256) k_lod_finish(int L, int n, int P, double*
 // ---------------------------------------------------------------------------------------------
 // Small control kernels.
 
-__global__ void k_d_arm(DScalars* S, unsigned long long handle) {
+__global__ void k_d_arm(DScalars* S, unsigned long long handle, unsigned long long handle_if) {
   S->cond = handle;
+  S->cond_if = handle_if;
   S->body_runs = 0;
   cudaGraphSetConditional((cudaGraphConditionalHandle)handle, S->stop == 0 ? 1u : 0u);
 }
-__global__ void k_d_disarm(DScalars* S) { S->cond = 0ull; }
+__global__ void k_d_disarm(DScalars* S) {
+  S->cond = 0ull;
+  S->cond_if = 0ull;
+}
 
 struct DProblem {
   double tol;
   int max_it, rule, n;
+  int reliable;  // the FP32 lane of DT_DIFF_MIXED_RELIABLE (its other fields from k_d_rel_init)
 };
 __global__ void k_d_begin(DScalars* S, DProblem p, int bb_from_dot) {
   S->tol = p.tol;
@@ -988,6 +1023,8 @@ __global__ void k_d_begin(DScalars* S, DProblem p, int bb_from_dot) {
   S->started = 0;
   S->body_runs = 0;
   S->cond = 0ull;
+  S->reliable = p.reliable;
+  S->gate_it = -1;
   if (!isfinite(S->rr) || !isfinite(S->bb))
     S->stop = DSTOP_NONFINITE;
   else if (!(S->rr > 0.0) || d_converged(S, S->rr))
@@ -1027,6 +1064,58 @@ __global__ void k_d_accumulate(size_t n, double* __restrict__ x, const float* __
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) x[k] += (double)x32[k] * inv;
 }
 __global__ void k_d_rr_is_bb(DScalars* S) { S->rr = S->bb; }
+
+// Reliable updates (the FP32 lane holds r32 = s r64 and its correction x32 = s e, s fixed from the
+// first residual's RMS). In an iteration that replaces the residual (gate_it == it):
+//   k_d_rel_accumulate                x64 += x32 / s; x32 = 0
+//   k_d_apply<.., DA_RESID_GATED>     r64 = b - A x64, ||r64||^2 -> rr_true
+//   k_d_rel_reset                     r32 = s r64 (and the cycle's copy); rr, maxrr from rr_true;
+//                                     stop when rr_true meets the tolerance
+__global__ void k_d_rel_accumulate(size_t n, double* __restrict__ x, float* __restrict__ x32, const double* scale,
+                                   const DScalars* S) {
+  if (S->stop || S->gate_it != S->it) return;
+  double inv = 1.0 / *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    x[k] += (double)x32[k] * inv;
+    x32[k] = 0.0f;
+  }
+}
+__global__ void k_d_rel_reset(size_t n, const double* __restrict__ r, float* __restrict__ r32, float* __restrict__ rm,
+                              const double* scale, DScalars* S) {
+  if (S->stop || S->gate_it != S->it) return;
+  double sc = *scale;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+    float v = (float)(r[k] * sc);
+    r32[k] = v;
+    rm[k] = v;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    double rr = S->rr_true * sc * sc;
+    S->rr = rr;
+    S->maxrr = rr;
+    S->replacements += 1;
+    if (!isfinite(S->rr_true)) {
+      S->stop = DSTOP_NONFINITE;
+    } else if (S->rr_true <= S->tol * S->tol * S->bb_true) {
+      S->stop = DSTOP_CONVERGED;
+    }
+    if (S->stop) dset_cond(S, 0);
+  }
+}
+// The FP32 lane's problem for reliable updates, from the FP64 lane's (bb, rr of r = b - A x) and
+// the scale s of r32 = s r: the tolerance on the relative residual, or with `rms` on the RMS
+// residual (||r||^2 <= tol^2 n).
+__global__ void k_d_rel_init(DScalars* F, const DScalars* S64, const double* scale, double delta, int rms) {
+  double s2 = (*scale) * (*scale);
+  double bref = rms ? (double)S64->n : S64->bb;
+  F->bb = bref * s2;
+  F->bb_true = bref;
+  F->rr = S64->rr * s2;
+  F->maxrr = F->rr;
+  F->delta2 = delta * delta;
+  F->replacements = 0;
+  F->cond_if = 0ull;
+}
 __global__ void k_convert_dr(size_t n, const double* __restrict__ a, float* __restrict__ b) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) b[k] = (float)a[k];
 }
@@ -1082,7 +1171,7 @@ struct dt_diff {
   dt::DScalars *S64 = nullptr, *S32 = nullptr;
   dt::Hier<float> hf[2];
   dt::Hier<double> hd[2];
-  dt::DGraph graph[3][2];
+  dt::DGraph graph[4][2];  // [lane: 0 split, 1 FP64, 2 FP32 inner, 3 FP32 reliable][cycle]
   // the Gauss-Seidel cycle's fused kernels (k_mg_rb2, k_mg_coarse_rb); DT_MG_FUSED=0 at create
   // keeps one launch per colour pass (the same values)
   bool mg_fused = true;
@@ -1256,24 +1345,83 @@ struct CgLane {
   TM* z;  // where the cycle leaves its result (set when the launch sequence is built)
 };
 
+// The residual replacement of a reliable-update iteration (the FP32 lane): gated kernels that do
+// nothing unless the iteration's update asked for it. `count`: count their launches (not inside
+// the loop body's IF node, whose runs are counted from the replacements).
+static void launch_reliable_d(dt_diff* s, Hier<float>& H, cudaStream_t st, bool count) {
+  unsigned int g = dgrid(s, s->n);
+  k_d_rel_accumulate<<<g, 256, 0, st>>>(s->n, s->x, s->x32, s->scale, s->S32);
+  k_d_apply<double, float, DA_RESID_GATED><<<g, 256, 0, st>>>(s->w, s->h, s->wrap && s->w > 1, s->east, s->south, s->diag, s->x,
+                                                              s->b, s->r, nullptr, s->partials, s->S32);
+  k_d_rel_reset<<<g, 256, 0, st>>>(s->n, s->r, s->r32, H.lv[0].r, s->scale, s->S32);
+  if (count)
+    for (int k = 0; k < 3; ++k) count_launch();
+}
+
+// While `st` captures a loop body: a conditional IF node, its body the residual replacement
+// (captured on `aside`), so that iterations that replace nothing launch nothing for it.
+static dt_status add_reliable_if_d(dt_diff* s, Hier<float>& H, cudaStream_t st, cudaStream_t aside,
+                                   unsigned long long* handle_out) {
+  cudaStreamCaptureStatus cs;
+  unsigned long long id = 0;
+  cudaGraph_t graph = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  DT_CUDA(cudaStreamGetCaptureInfo(st, &cs, &id, &graph, &deps, &nd));
+  if (cs != cudaStreamCaptureStatusActive || !graph) {
+    set_error("diffusion loop graph: the stream is not capturing");
+    return DT_DEVICE_ERROR;
+  }
+  cudaGraphConditionalHandle h;
+  DT_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 0, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  DT_CUDA(cudaGraphAddNode(&node, graph, deps, nd, &cp));
+  DT_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+  DT_CUDA(cudaStreamBeginCaptureToGraph(aside, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                        cudaStreamCaptureModeThreadLocal));
+  launch_reliable_d(s, H, aside, false);
+  cudaGraph_t ifbody;
+  DT_CUDA(cudaStreamEndCapture(aside, &ifbody));
+  *handle_out = (unsigned long long)h;
+  return DT_OK;
+}
+
+// One CG iteration (multigrid.rs:698-733). With `reliable` (the FP32 lane of
+// DT_DIFF_MIXED_RELIABLE) the residual replacement follows the update: under an IF node when
+// `aside` is given (capturing a loop body; its handle goes to *if_handle), else launched gated.
 template <class TC, class TM>
-static void cg_iteration(dt_diff* s, CgLane<TC, TM>& C, int kind, cudaStream_t st) {
+static dt_status cg_iteration(dt_diff* s, CgLane<TC, TM>& C, int kind, cudaStream_t st, bool reliable = false,
+                              cudaStream_t aside = nullptr, unsigned long long* if_handle = nullptr) {
   unsigned int g = dgrid(s, s->n);
   k_d_apply<TC, TM, DA_PAP><<<g, 256, 0, st>>>(s->w, s->h, s->wrap && s->w > 1, C.east, C.south, C.diag, C.p, nullptr, C.ap,
                                                 nullptr, s->partials, C.S);
   count_launch();
   k_d_update<TC, TM><<<g, 256, 0, st>>>(s->n, C.x, C.r, C.H->lv[0].r, C.p, C.ap, s->partials, C.S);
   count_launch();
+  if constexpr (std::is_same<TM, float>::value) {
+    if (reliable) {
+      if (aside)
+        DT_TRY(add_reliable_if_d(s, *C.H, st, aside, if_handle));
+      else
+        launch_reliable_d(s, *C.H, st, true);
+    }
+  }
   TM* z = vcycle<TM>(s, *C.H, 0, kind, st);
   C.z = z;
   k_d_rz<TC, TM><<<g, 256, 0, st>>>(s->n, C.r, z, s->partials, C.S);
   count_launch();
   k_d_direction<TC, TM><<<g, 256, 0, st>>>(s->n, C.p, z, C.S, 0);
   count_launch();
+  return DT_OK;
 }
 
 template <class TC, class TM>
-static dt_status cg_graph(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, DGraph** out) {
+static dt_status cg_graph(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, DGraph** out, bool reliable = false) {
   DGraph& G = s->graph[lane][kind];
   if (G.exec) {
     *out = &G;
@@ -1283,10 +1431,10 @@ static dt_status cg_graph(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, DGr
   DT_CUDA(cudaGraphCreate(&g, 0));
   cudaGraphConditionalHandle handle;
   DT_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
-  unsigned long long hv = (unsigned long long)handle;
+  unsigned long long hv = (unsigned long long)handle, hv_if = 0ull;
   DScalars* Sp = C.S;
   cudaKernelNodeParams kp = {};
-  void* arm_args[] = {&Sp, &hv};
+  void* arm_args[] = {&Sp, &hv, &hv_if};
   kp.func = (void*)k_d_arm;
   kp.gridDim = dim3(1);
   kp.blockDim = dim3(1);
@@ -1300,12 +1448,18 @@ static dt_status cg_graph(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, DGr
   cp.conditional.size = 1;
   DT_CUDA(cudaGraphAddNode(&n_loop, g, &n_arm, 1, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t aside = nullptr;
+  if (reliable) DT_CUDA(cudaStreamCreateWithFlags(&aside, cudaStreamNonBlocking));
   DT_CUDA(cudaStreamBeginCaptureToGraph(s->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   begin_capture_count();
-  cg_iteration<TC, TM>(s, C, kind, s->stream);
+  dt_status st_body = cg_iteration<TC, TM>(s, C, kind, s->stream, reliable, aside, &hv_if);
   G.body_kernels = end_capture_count();
   cudaGraph_t captured;
-  DT_CUDA(cudaStreamEndCapture(s->stream, &captured));
+  cudaError_t e_end = cudaStreamEndCapture(s->stream, &captured);
+  if (aside) cudaStreamDestroy(aside);
+  DT_TRY(st_body);
+  DT_CUDA(e_end);
+  if (reliable) DT_CUDA(cudaGraphKernelNodeSetParams(n_arm, &kp));  // k_d_arm learns the IF node's handle
   void* dis_args[] = {&Sp};
   kp.func = (void*)k_d_disarm;
   kp.kernelParams = dis_args;
@@ -1324,7 +1478,8 @@ static dt_status dread(dt_diff* s, const DScalars* S, DScalars* out) {
 
 // CG of lane C from x with r = b - A x, rm and S->rr, S->bb already set.
 template <class TC, class TM>
-static dt_status run_cg(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, const DProblem& prob, int host_loop, DScalars* out) {
+static dt_status run_cg(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, const DProblem& prob, int host_loop, DScalars* out,
+                        bool reliable = false) {
   cudaStream_t st = s->stream;
   unsigned int g = dgrid(s, s->n);
   k_d_begin<<<1, 1, 0, st>>>(C.S, prob, 0);
@@ -1337,7 +1492,7 @@ static dt_status run_cg(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, const
   count_launch();
   if (!host_loop) {
     DGraph* G;
-    DT_TRY(cg_graph<TC, TM>(s, C, lane, kind, &G));
+    DT_TRY(cg_graph<TC, TM>(s, C, lane, kind, &G, reliable));
     DT_CUDA(cudaGraphLaunch(G->exec, st));
     DT_TRY(dread(s, C.S, out));
     add_launches(2 + G->body_kernels * (long long)out->body_runs);
@@ -1345,7 +1500,7 @@ static dt_status run_cg(dt_diff* s, CgLane<TC, TM>& C, int lane, int kind, const
   }
   DT_TRY(dread(s, C.S, out));
   for (int pass = 0; pass < prob.max_it + 2 && out->stop == DSTOP_RUNNING; ++pass) {
-    cg_iteration<TC, TM>(s, C, kind, st);
+    DT_TRY(cg_iteration<TC, TM>(s, C, kind, st, reliable));
     DT_CUDA(cudaGetLastError());
     DT_TRY(dread(s, C.S, out));
     if (host_loop > 1)
@@ -1499,6 +1654,43 @@ static dt_status solve_mixed_cg(dt_diff* s, const dt_diff_params* p, dt_report* 
   return DT_OK;
 }
 
+// One FP32 CG (FP32 cycle) with reliable updates: the residual scaled to unit RMS once, then
+// replaced by the FP64 b - A x (x folded into the FP64 accumulation) each time the FP32 residual
+// has fallen a hundredfold or meets the tolerance; the FP64 residual alone decides convergence, and the
+// search direction carries on, so the Krylov space is never restarted.
+static dt_status solve_mixed_reliable(dt_diff* s, const dt_diff_params* p, dt_report* rep, DScalars* fin) {
+  cudaStream_t st = s->stream;
+  Hier<float>& H = s->hf[p->cycle];
+  DT_TRY(build_levels<float>(s, H, p->cycle == DT_CYCLE_JACOBI ? COARSEST : COARSEST_GS));
+  fill_levels<float>(s, H, p->cycle, st);
+  unsigned int g = dgrid(s, s->n);
+  int wrap = s->wrap && s->w > 1;
+  k_d_dot<double><<<g, 256, 0, st>>>(s->n, s->b, s->b, s->partials, s->S64);
+  k_d_begin<<<1, 1, 0, st>>>(s->S64, DProblem{p->tol, p->max_iterations, p->stop, (int)s->n}, 1);
+  k_d_apply<double, float, DA_RESID><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->x, s->b, s->r, s->r32,
+                                                        s->partials, s->S64);
+  k_d_scale_down<<<g, 256, 0, st>>>(s->n, s->r, s->r32, s->x32, s->S64, s->scale);
+  // replace when the FP32 residual has fallen a hundredfold: the V-cycle cuts it more than
+  // tenfold an iteration, so a tenfold trigger would replace it every iteration
+  k_d_rel_init<<<1, 1, 0, st>>>(s->S32, s->S64, s->scale, 0.01, p->stop == DT_STOP_RMS_RESIDUAL);
+  DT_CUDA(cudaMemcpyAsync(H.lv[0].r, s->r32, s->n * sizeof(float), cudaMemcpyDeviceToDevice, st));  // the cycle's rhs
+  for (int k = 0; k < 6; ++k) count_launch();
+  CgLane<float, float> C{s->x32, s->r32, s->p32, s->ap32, s->east32, s->south32, s->diag32, &H, s->S32, nullptr};
+  DScalars h32;
+  DT_TRY(run_cg<float, float>(s, C, 3, p->cycle, DProblem{p->tol, p->max_iterations, DT_STOP_REL_RESIDUAL, (int)s->n, 1},
+                              p->host_loop, &h32, true));
+  if (!p->host_loop) add_launches(3LL * h32.replacements);
+  // the correction since the last replacement (zero when the solve ended on one)
+  k_d_accumulate<<<g, 256, 0, st>>>(s->n, s->x, s->x32, s->scale);
+  count_launch();
+  *fin = h32;
+  if (rep) {
+    rep->iterations = h32.it;
+    rep->refinements = h32.replacements;
+  }
+  return DT_OK;
+}
+
 }  // namespace dt
 
 using namespace dt;
@@ -1620,7 +1812,7 @@ static dt_status diff_check(const dt_diff_params* p, double dt) {
     set_error("diffusion solve: params is NULL");
     return DT_BAD_ARG;
   }
-  if ((p->cycle != DT_CYCLE_JACOBI && p->cycle != DT_CYCLE_RBGS) || p->precision < 0 || p->precision > 2 ||
+  if ((p->cycle != DT_CYCLE_JACOBI && p->cycle != DT_CYCLE_RBGS) || p->precision < 0 || p->precision > 3 ||
       (p->stop != DT_STOP_RMS_RESIDUAL && p->stop != DT_STOP_REL_RESIDUAL) || !(p->tol >= 0.0) || p->max_iterations < 0) {
     set_error("diffusion solve: bad parameters (cycle %d, precision %d, rule %d, tol %g)", p->cycle, p->precision, p->stop, p->tol);
     return DT_BAD_ARG;
@@ -1647,6 +1839,8 @@ static dt_status diff_solve_loaded(dt_diff* s, double dt, const dt_diff_params* 
   if (rep) memset(rep, 0, sizeof *rep);
   if (p->precision == DT_DIFF_MIXED) {
     DT_TRY(solve_mixed_cg(s, p, rep, &fin));
+  } else if (p->precision == DT_DIFF_MIXED_RELIABLE) {
+    DT_TRY(solve_mixed_reliable(s, p, rep, &fin));
   } else if (p->precision == DT_DIFF_FP64) {
     DT_TRY(solve_fp64_cg<double>(s, p, 1, rep, &fin));
   } else {

@@ -16,7 +16,7 @@ STOP_MAX_Z, STOP_REL_RESIDUAL, STOP_RMS_RESIDUAL = 0, 1, 2
 PREC_FP64, PREC_MIXED, PREC_MIXED_RELIABLE = 0, 1, 2
 WARM_NONE, WARM_GIVEN, WARM_UNET = 0, 1, 2
 CYCLE_JACOBI, CYCLE_RBGS = 0, 1
-DIFF_FP64_CG_FP32_CYCLE, DIFF_FP64, DIFF_MIXED = 0, 1, 2
+DIFF_FP64_CG_FP32_CYCLE, DIFF_FP64, DIFF_MIXED, DIFF_MIXED_RELIABLE = 0, 1, 2, 3
 
 
 class FlexParams(ctypes.Structure):

@@ -60,7 +60,8 @@ enum { DT_CYCLE_JACOBI = 0,      /* the reference's V-cycle: damped Jacobi, omeg
        DT_CYCLE_RBGS = 1 };      /* red-black Gauss-Seidel V(2,2) to a 16 x 8 coarsest level */
 enum { DT_DIFF_FP64_CG_FP32_CYCLE = 0, /* the reference's split: FP64 CG, FP32 cycle */
        DT_DIFF_FP64 = 1,               /* FP64 CG and FP64 cycle */
-       DT_DIFF_MIXED = 2 };            /* FP32 inner CG + FP32 cycle inside FP64 refinement */
+       DT_DIFF_MIXED = 2,              /* FP32 inner CG + FP32 cycle inside FP64 refinement */
+       DT_DIFF_MIXED_RELIABLE = 3 };   /* one FP32 CG + FP32 cycle, FP64 reliable updates of x and r */
 
 typedef struct {
   int precond;          /* DT_PRECOND_* */
@@ -148,7 +149,8 @@ dt_status dt_flex_operator_dot_noalloc(int w, int h, double dx, const double* d,
 
 typedef struct {
   int cycle;            /* DT_CYCLE_JACOBI (the reference's, default) or DT_CYCLE_RBGS */
-  int precision;        /* DT_DIFF_FP64_CG_FP32_CYCLE (the reference's, default), DT_DIFF_FP64, DT_DIFF_MIXED */
+  int precision;        /* DT_DIFF_FP64_CG_FP32_CYCLE (the reference's, default), DT_DIFF_FP64, DT_DIFF_MIXED,
+                           DT_DIFF_MIXED_RELIABLE */
   int stop;             /* DT_STOP_RMS_RESIDUAL (the reference's: RMS residual < tol metres) or DT_STOP_REL_RESIDUAL */
   double tol;           /* default 1e-5 m (surface.numerics.diffusion_tol_m, params.rs:197-200) */
   int max_iterations;   /* default 400 (CG_MAX_ITER, diffusion.rs:497) */

@@ -109,7 +109,7 @@ def test_the_cycle_takes_far_fewer_iterations_than_jacobi_on_a_shelf():
     assert 3 * rep.iterations <= jac, (rep.iterations, jac)
 
 
-@pytest.mark.parametrize("precision", [L.DIFF_FP64_CG_FP32_CYCLE, L.DIFF_FP64, L.DIFF_MIXED])
+@pytest.mark.parametrize("precision", [L.DIFF_FP64_CG_FP32_CYCLE, L.DIFF_FP64, L.DIFF_MIXED, L.DIFF_MIXED_RELIABLE])
 @pytest.mark.parametrize("cycle", [L.CYCLE_JACOBI, L.CYCLE_RBGS])
 def test_baseline_variants_reach_the_fp64_answer(precision, cycle):
     # the 2048 x 1024 workload's recipe at 512 x 256: rel. residual 1e-10 against the oracle's
@@ -125,6 +125,28 @@ def test_baseline_variants_reach_the_fp64_answer(precision, cycle):
     assert rep.converged and rep.rel_residual < 2e-10, rep
     assert rel_l2(x, exact) < 1e-8
     assert abs(x.sum() - topo.sum()) <= 1e-9 * np.abs(topo).sum()
+
+
+@pytest.mark.parametrize("stop,tol", [(L.STOP_REL_RESIDUAL, 1e-10), (L.STOP_RMS_RESIDUAL, 1e-6)])
+def test_reliable_updates_keep_the_fp64_iteration_count(stop, tol):
+    # one FP32 CG whose residual the FP64 b - A x replaces (no restart): no more iterations than
+    # FP64 CG plus one, fewer than or as many as FP32 refinement, and the device loop the same
+    # iterations and bits as the same kernels driven from the host
+    w, h = 512, 256
+    topo, s = I.diffusion_problem(w, h, 8.0, 4400)
+    kd = s * 1e6
+    ws = D.Workspace(D.Dims(w, h, 1000.0, True))
+    its = {}
+    for name, prec in (("fp64", L.DIFF_FP64), ("refine", L.DIFF_MIXED), ("reliable", L.DIFF_MIXED_RELIABLE)):
+        x, rep = ws.solve_with(topo, kd, 1.0, D.params(cycle=L.CYCLE_RBGS, precision=prec, stop=stop, tol=tol))
+        assert rep.converged, (name, rep)
+        its[name] = rep.iterations
+    assert its["reliable"] <= its["fp64"] + 1 and its["reliable"] <= its["refine"], its
+    xg, rg = ws.solve_with(topo, kd, 1.0, D.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_MIXED_RELIABLE, stop=stop, tol=tol))
+    xh, rh = ws.solve_with(topo, kd, 1.0, D.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_MIXED_RELIABLE, stop=stop, tol=tol,
+                                                   host_loop=1))
+    assert rg.iterations == rh.iterations and rg.refinements == rh.refinements >= 1, (rg, rh)
+    assert np.array_equal(xg, xh)
 
 
 def test_the_red_black_cycle_needs_fewer_iterations():
@@ -170,7 +192,7 @@ def test_the_fused_gauss_seidel_cycle_is_bit_for_bit_the_per_colour_launches(w, 
         assert lf == la and np.array_equal(zf, za), float(np.abs(zf - za).max())
     # solves: the mixed one's FP32 cycle is bit for bit; in FP64 the compiler forms fused
     # multiply-adds differently in the two kernels, so the answers agree to 1e-12 relative
-    for precision in (L.DIFF_FP64, L.DIFF_MIXED):
+    for precision in (L.DIFF_FP64, L.DIFF_MIXED, L.DIFF_MIXED_RELIABLE):
         p = D.params(cycle=L.CYCLE_RBGS, precision=precision, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000)
         xf, rf = fused.solve_with(z0, kd, 2.0e6, p)
         xa, ra = apart.solve_with(z0, kd, 2.0e6, p)

@@ -5,7 +5,8 @@ first guess gains.
   a smoothed log-uniform field over [0.1, 100]): red-black Gauss-Seidel V(2,2) multigrid CG to
   relative residual 1e-10, FP64 and FP32-cycle/FP64-refinement, and the reference's own split
   (FP64 CG, FP32 damped-Jacobi cycle), against the oracle's unpreconditioned CG to 1e-13
-  (multigrid/tests.rs:17-74's oracle). Bound: relative L2 <= 1e-8, max-abs <= 1e-8 of max |h'|.
+  (multigrid/tests.rs:17-74's oracle), and one FP32 CG with FP64 reliable updates on the same
+  cycle. Bound: relative L2 <= 1e-8, max-abs <= 1e-8 of max |h'|.
 - Flexure, 4096 x 2048 (dx 2.5 km, rigidity smoothed over 32 cells): the benchmarked method (FP32
   PCG with FP64 reliable updates, the reference preconditioner, the U-Net's first guess when the
   trained weights are present) and the plain FP64 mean-D method to relative residual 1e-8,
@@ -48,6 +49,7 @@ def diffusion_case():
 
 @pytest.mark.parametrize("name,cycle,precision", [("fp64_rbgs", L.CYCLE_RBGS, L.DIFF_FP64),
                                                   ("mixed_rbgs", L.CYCLE_RBGS, L.DIFF_MIXED),
+                                                  ("mixed_reliable_rbgs", L.CYCLE_RBGS, L.DIFF_MIXED_RELIABLE),
                                                   ("reference_split", L.CYCLE_JACOBI, L.DIFF_FP64_CG_FP32_CYCLE)])
 def test_the_diffusion_config_at_full_size_matches_the_oracle(diffusion_case, name, cycle, precision):
     w, h, dx, dt, topo, kd, exact = diffusion_case

@@ -66,7 +66,7 @@ def test_diffusion_operator_and_solves(diff):
     x, rep = ws.solve_with(h0, kd, 1000.0, D.params(tol=1e-5))
     assert abs(rep.iterations - int(diff["iterations_reference_rule"])) <= 1
     assert np.sqrt(np.mean((x.reshape(h0.shape) - diff["h_reference_rule"]) ** 2)) <= 1e-5
-    for precision in (L.DIFF_FP64, L.DIFF_MIXED):
+    for precision in (L.DIFF_FP64, L.DIFF_MIXED, L.DIFF_MIXED_RELIABLE):
         p = D.params(precision=precision, stop=L.STOP_REL_RESIDUAL, tol=1e-12)
         x, rep = ws.solve_with(h0, kd, 1000.0, p)
         assert rep.converged and rel(x.reshape(h0.shape), diff["h_rel_1e-12"]) <= 1e-8, (precision, rep)
