@@ -258,16 +258,6 @@ __device__ __forceinline__ void thomas_line(int n, size_t base, size_t stride, c
   }
 }
 
-// Face rows in transposed order: thread (f, j) walks i at f n^2 + i n + j
-__global__ void k_cube_lod_rows_t(int n, const double* __restrict__ loT, const double* __restrict__ upT,
-                                  const double* __restrict__ diT, const double* __restrict__ bT, double* __restrict__ xT,
-                                  double* __restrict__ cT) {
-  const int row = blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= 6 * n) return;
-  const size_t nn = (size_t)n * n, f = row / n, j = row % n;
-  thomas_line(n, f * nn + j, (size_t)n, loT, upT, diT, bT, xT, cT);
-}
-
 // Face columns in the cells' order: thread (f, i) walks j at f n^2 + j n + i; the right-hand
 // side y plus the couplings across the face's north and south edges at y's values (into rhs)
 __global__ void k_cube_lod_cols_rhs(int n, const uint32_t* __restrict__ slots, const double* __restrict__ k,
@@ -281,6 +271,8 @@ __global__ void k_cube_lod_cols_rhs(int n, const uint32_t* __restrict__ slots, c
     rhs[c] = v;
   }
 }
+// One serial walk a line (the rows' transposed systems and the columns' alike: line l = f n + m
+// at f n^2 + m + r n): the comparison path of the chunked solves below.
 __global__ void k_cube_lod_cols_f(int n, const double* __restrict__ lo, const double* __restrict__ up,
                                   const double* __restrict__ di, const double* __restrict__ rhs, double* __restrict__ x,
                                   double* __restrict__ c) {
@@ -288,6 +280,116 @@ __global__ void k_cube_lod_cols_f(int n, const double* __restrict__ lo, const do
   if (col >= 6 * n) return;
   const size_t nn = (size_t)n * n, f = col / n, i = col % n;
   thomas_line(n, f * nn + i, (size_t)n, lo, up, di, rhs, x, c);
+}
+
+// The same line solves in chunks, for parallelism: the 6 n lines of n positions at
+// f n^2 + m + r n (line l = f n + m, r = 0 .. n - 1) in chunks of CUBE_LOD_CHUNK positions, one
+// thread a chunk. With the couplings to the neighbouring chunks moved to the right-hand side,
+// x_i = p_i + q_i x_(s-1) + r_i x_e on chunk [s, e): p, q and r solve the chunk's own tridiagonal
+// system for the right-hand sides b, -lo_s e_s and -up_(e-1) e_(e-1) (a line's first lo and last
+// up couple nothing). k_cube_lod_reduce then solves each line's chunk end values, one thread a
+// line, and k_cube_lod_join forms x over p. Every product, quotient and difference is rounded on
+// its own, as in thomas_line.
+constexpr int CUBE_LOD_CHUNK = 32;
+__global__ void __launch_bounds__(128) k_cube_lod_chunks(int n, int P, const double* __restrict__ lo, const double* __restrict__ up,
+                                                         const double* __restrict__ di, const double* __restrict__ rhs,
+                                                         double* __restrict__ p, double* __restrict__ q, double* __restrict__ r,
+                                                         double* __restrict__ c, double* __restrict__ edge) {
+  const int L = 6 * n;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= L * P) return;
+  const int l = t % L, k = t / L;  // consecutive threads: consecutive lines, consecutive words
+  const size_t base = (size_t)(l / n) * n * n + (size_t)(l % n);
+  const int s = k * CUBE_LOD_CHUNK, e = min(s + CUBE_LOD_CHUNK, n);
+  double bt = 1.0, cprev = 0.0, pv = 0.0, qv = 0.0, rv = 0.0;
+  for (int i = s; i < e; ++i) {
+    const size_t a = base + (size_t)i * n;
+    const double lov = i == 0 ? 0.0 : lo[a];
+    const double upv = i == n - 1 ? 0.0 : up[a];
+    const double dv = di[a], bv = rhs[a];
+    const double rr = i == e - 1 ? -upv : 0.0;
+    if (i == s) {
+      bt = dv;
+      pv = __ddiv_rn(bv, bt);
+      qv = __ddiv_rn(-lov, bt);
+      rv = __ddiv_rn(rr, bt);
+    } else {
+      bt = __dsub_rn(dv, __dmul_rn(lov, cprev));
+      pv = __ddiv_rn(__dsub_rn(bv, __dmul_rn(lov, pv)), bt);
+      qv = __ddiv_rn(-__dmul_rn(lov, qv), bt);
+      rv = __ddiv_rn(__dsub_rn(rr, __dmul_rn(lov, rv)), bt);
+    }
+    cprev = __ddiv_rn(upv, bt);
+    c[a] = cprev;
+    p[a] = pv;
+    q[a] = qv;
+    r[a] = rv;
+  }
+  // back substitution inside the chunk: y_i -= c_i y_(i+1) (the last position's values are final)
+  const double e0 = pv, eq = qv, er = rv;
+  for (int i = e - 2; i >= s; --i) {
+    const size_t a = base + (size_t)i * n;
+    const double ci = c[a];
+    pv = __dsub_rn(p[a], __dmul_rn(ci, pv));
+    qv = __dsub_rn(q[a], __dmul_rn(ci, qv));
+    rv = __dsub_rn(r[a], __dmul_rn(ci, rv));
+    p[a] = pv;
+    q[a] = qv;
+    r[a] = rv;
+  }
+  double* ed = edge + (size_t)t * 6;  // the chunk's first position's p, q, r, then its last's
+  ed[0] = pv;
+  ed[1] = qv;
+  ed[2] = rv;
+  ed[3] = e0;
+  ed[4] = eq;
+  ed[5] = er;
+}
+
+// One thread a line: the chunks' first (A_k) and last (B_k) values from A_k = pA + qA B_(k-1) +
+// rA A_(k+1) and B_k = pB + qB B_(k-1) + rB A_(k+1) (B_(-1) = A_P = 0): forward with
+// B_(k-1) = g + hh A_k, back from A_P; A_k and B_k written over the chunk's p entries.
+__global__ void __launch_bounds__(128) k_cube_lod_reduce(int n, int P, double* __restrict__ edge, double* __restrict__ al) {
+  const int L = 6 * n;
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= L) return;
+  double g = 0.0, hh = 0.0;
+  for (int k = 0; k < P; ++k) {
+    const double* ed = edge + ((size_t)k * L + l) * 6;
+    const double pA = ed[0], qA = ed[1], rA = ed[2], pB = ed[3], qB = ed[4], rB = ed[5];
+    const double d = __dsub_rn(1.0, __dmul_rn(qA, hh));
+    const double a = __ddiv_rn(__dadd_rn(pA, __dmul_rn(qA, g)), d), be = __ddiv_rn(rA, d);
+    double* sk = al + ((size_t)k * L + l) * 4;
+    sk[0] = a;
+    sk[1] = be;
+    g = __dadd_rn(__dadd_rn(pB, __dmul_rn(qB, g)), __dmul_rn(__dmul_rn(qB, hh), a));
+    hh = __dadd_rn(__dmul_rn(__dmul_rn(qB, hh), be), rB);
+    sk[2] = g;
+    sk[3] = hh;
+  }
+  double An = 0.0;
+  for (int k = P - 1; k >= 0; --k) {
+    const double* sk = al + ((size_t)k * L + l) * 4;
+    const double A = __dadd_rn(sk[0], __dmul_rn(sk[1], An)), B = __dadd_rn(sk[2], __dmul_rn(sk[3], An));
+    double* ed = edge + ((size_t)k * L + l) * 6;
+    ed[0] = A;
+    ed[3] = B;
+    An = A;
+  }
+}
+
+// Every position: x = p + q B_(k-1) + r A_(k+1), over p.
+__global__ void __launch_bounds__(256) k_cube_lod_join(int n, int P, double* __restrict__ p, const double* __restrict__ q,
+                                                       const double* __restrict__ r, const double* __restrict__ edge) {
+  const int L = 6 * n;
+  const size_t nn = (size_t)n * n, cells = 6 * nn;
+  for (size_t a = blockIdx.x * (size_t)blockDim.x + threadIdx.x; a < cells; a += (size_t)gridDim.x * blockDim.x) {
+    const size_t f = a / nn, rest = a % nn;
+    const int i = (int)(rest / n), l = (int)(f * n + rest % n), k = i / CUBE_LOD_CHUNK;
+    const double Bm = k > 0 ? edge[((size_t)(k - 1) * L + l) * 6 + 3] : 0.0;
+    const double Ap = k + 1 < P ? edge[((size_t)(k + 1) * L + l) * 6 + 0] : 0.0;
+    p[a] = __dadd_rn(__dadd_rn(p[a], __dmul_rn(q[a], Bm)), __dmul_rn(r[a], Ap));
+  }
 }
 
 // x (face row-major) from the column pass's face-column-major result
@@ -407,13 +509,13 @@ __device__ __forceinline__ float mg_az_plain(unsigned i, const MgLevelDev& L, co
 }
 
 __global__ void __launch_bounds__(1024) k_mg_coarse_cycle(MgCoarse m) {
+  const unsigned tid = threadIdx.x, nt = blockDim.x;
   float* z[CUBE_MAX_FUSED];
   float* t[CUBE_MAX_FUSED];
   for (int l = 0; l < m.count; ++l) {
     z[l] = m.lv[l].z;
     t[l] = m.lv[l].t;
   }
-  const unsigned tid = threadIdx.x, nt = blockDim.x;
   auto sweep = [&](int l, bool first) {
     const MgLevelDev& L = m.lv[l];
     if (first) {
@@ -608,6 +710,10 @@ struct dt_cube {
   double *k = nullptr, *s = nullptr, *diag = nullptr;
   double *rhs = nullptr, *x = nullptr, *b = nullptr, *tmp = nullptr, *cb = nullptr;
   double* lodw[7] = {};  // the LOD's row systems (transposed) and column systems
+  // the chunked line solves' scratch: q, r (a value a cell), the chunks' end records (6 a chunk)
+  // and the reduction's (4 a chunk); DT_CUBE_LOD_CHUNKED=0 at create keeps one serial walk a line
+  double *lq = nullptr, *lr = nullptr, *ledge = nullptr, *lal = nullptr;
+  bool lod_chunked = true;
   double *r = nullptr, *z = nullptr, *po = nullptr, *pn = nullptr, *ap = nullptr;
   double* partials = nullptr;
   double* sc = nullptr;  // scalars: 0 rr, 1 pap, 2 rz, 3 rz_new, 4 alpha, 5 beta, 6 lost, 7 weight, 8 kk, 9 rhs.rhs,
@@ -767,10 +873,22 @@ void cube_lod(dt_cube* s, const double* b, double* x) {
   // the systems laid out for contiguous walks; the rows' answer comes back transposed in tmp
   k_cube_lod_prep<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, b, w[0], w[1], w[2], w[3], w[4],
                                                               w[5], w[6]);
-  k_cube_lod_rows_t<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, w[0], w[1], w[2], w[3], s->tmp, s->cb);
+  const int P = (s->n + CUBE_LOD_CHUNK - 1) / CUBE_LOD_CHUNK;
+  // one pass of line solves: x over the lines' systems (lo, up, di, rhs)
+  auto lines = [&](const double* lo, const double* up, const double* di, const double* rhs, double* out) {
+    if (!s->lod_chunked) {
+      k_cube_lod_cols_f<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, lo, up, di, rhs, out, s->cb);
+      return;
+    }
+    k_cube_lod_chunks<<<ceil_div((size_t)rows * P, 128), 128, 0, s->stream>>>(s->n, P, lo, up, di, rhs, out, s->lq, s->lr, s->cb,
+                                                                             s->ledge);
+    k_cube_lod_reduce<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, P, s->ledge, s->lal);
+    k_cube_lod_join<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, P, out, s->lq, s->lr, s->ledge);
+  };
+  lines(w[0], w[1], w[2], w[3], s->tmp);
   k_cube_untranspose<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->tmp, x);
   k_cube_lod_cols_rhs<<<cube_grid(s->cells), 256, 0, s->stream>>>(s->n, s->slots, s->k, s->mu, x, w[3]);
-  k_cube_lod_cols_f<<<ceil_div(rows, 128), 128, 0, s->stream>>>(s->n, w[4], w[5], w[6], w[3], x, s->cb);
+  lines(w[4], w[5], w[6], w[3], x);
 }
 
 // One device scalar to the host (a sync); a device error reads as NaN, which ends the loop and
@@ -1082,6 +1200,14 @@ dt_status dt_cube_create(int n, const uint32_t* slots, const double* lap, const 
     if ((st = cube_alloc(s, p, cells)) != DT_OK) return fail(st);
   for (double*& p : s->lodw)
     if ((st = cube_alloc(s, &p, cells)) != DT_OK) return fail(st);
+  {
+    const size_t chunks = (size_t)6 * n * ((n + CUBE_LOD_CHUNK - 1) / CUBE_LOD_CHUNK);
+    for (double** p : {&s->lq, &s->lr})
+      if ((st = cube_alloc(s, p, cells)) != DT_OK) return fail(st);
+    if ((st = cube_alloc(s, &s->ledge, chunks * 6)) != DT_OK) return fail(st);
+    if ((st = cube_alloc(s, &s->lal, chunks * 4)) != DT_OK) return fail(st);
+  }
+  if (const char* e = std::getenv("DT_CUBE_LOD_CHUNKED")) s->lod_chunked = e[0] != '0';
   if ((st = cube_alloc(s, &s->partials, 2 * CUBE_RED_BLOCKS)) != DT_OK) return fail(st);
   if ((st = cube_alloc(s, &s->sc, 16)) != DT_OK) return fail(st);
   // the hierarchy (multigrid.rs:170-186): coarsen while a level has more than 64 cells and a side

@@ -38,6 +38,24 @@ def test_lod_first_guess_matches_the_oracle(case):
     assert rel(dev.lod(kd, 7.0, h), O.cube_lod(n, slots, lap, areas, kd, 7.0, h)) < 1e-14
 
 
+@pytest.mark.parametrize("n", [33, 70, 256])
+def test_the_chunked_line_solves_match_the_serial_walks_and_the_oracle(n, monkeypatch):
+    # lines of n cells in chunks of 32 (two with a last chunk of one cell, three with a ragged
+    # last, eight) against one serial walk a line (DT_CUBE_LOD_CHUNKED=0 at create) and the oracle
+    slots = O.cube_topology(n)
+    lap, areas, kd, h = cube_case(n, n + 100, slots)
+    chunked = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.setenv("DT_CUBE_LOD_CHUNKED", "0")
+    serial = C.CubeDiffusion(n, slots, lap, areas)
+    monkeypatch.delenv("DT_CUBE_LOD_CHUNKED")
+    want = O.cube_lod(n, slots, lap, areas, kd, 7.0, h)
+    got, walk = chunked.lod(kd, 7.0, h), serial.lod(kd, 7.0, h)
+    assert rel(walk, want) < 1e-14
+    assert rel(got, want) < 1e-14 and rel(got, walk) < 1e-14, (rel(got, want), rel(got, walk))
+    chunked.close()
+    serial.close()
+
+
 def test_vcycle_matches_the_oracle(case):
     n, slots, lap, areas, kd, h, dev = case
     r = np.random.default_rng(2).standard_normal(6 * n * n)
