@@ -103,6 +103,11 @@ def parse():
                     help="profiling aid (for ncu): run one host-driven, iteration-capped solve and exit; "
                          "'W,H,DX,PRECOND,PRECISION,ITERATIONS' with PRECOND 0 reference / 1 mean-D and PRECISION "
                          "0 fp64 / 1 FP32 inside FP64 refinement / 2 FP32 with FP64 reliable updates")
+    ap.add_argument("--diff-case", default=None,
+                    help="profiling aid (for ncu): run one host-driven diffusion solve of the 2048 x 1024 workload's "
+                         "recipe (red-black V(2,2), relative residual 1e-10) and exit; 'W,H,PRECISION' with PRECISION "
+                         "0 the reference's split / 1 fp64 / 2 FP32 inside FP64 refinement / 3 FP32 with FP64 "
+                         "reliable updates")
     return ap.parse_args()
 
 
@@ -118,6 +123,27 @@ def run_case(spec):
     p = F.params(precond=pc, stop=L.STOP_REL_RESIDUAL, precision=prec, tol=TOL, max_iterations=its, host_loop=1)
     x, rep = sv.solve_with(d, c, b, p)
     print(rep, flush=True)
+
+
+def run_diff_case(spec):
+    import torch
+
+    from deeptime_gpu import _lib as L
+    from deeptime_gpu import diffusion as D
+    from deeptime_gpu import inputs as I
+
+    w, h, prec = (int(v) for v in spec.split(","))
+    dx, dt = 10_000.0, 1.0
+    h0, s = I.diffusion_problem(w, h, 8.0, 3000)
+    ws = D.Workspace(D.Dims(w, h, dx, True))
+    x, kd = torch.from_numpy(h0).cuda(), torch.from_numpy(s * dx * dx / dt).cuda()
+    cycle = L.CYCLE_JACOBI if prec == L.DIFF_FP64_CG_FP32_CYCLE else L.CYCLE_RBGS
+    p = D.params(cycle=cycle, precision=prec, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000, host_loop=1)
+    rep = L.Report()
+    L.check(L.lib().dt_diff_solve_dev(ws._h, ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(kd.data_ptr()),
+                                      ctypes.c_double(dt), ctypes.byref(p), ctypes.byref(rep)))
+    print(f"iterations {rep.iterations}, converged {bool(rep.converged)}, relative residual {rep.rel_residual:.3e}, "
+          f"refinements or replacements {rep.refinements}", flush=True)
 
 
 def dist_init(n, timeout_s=300):
@@ -511,6 +537,9 @@ def launch_ranks(args):
 
 def main():
     args = parse()
+    if args.diff_case:
+        run_diff_case(args.diff_case)
+        return
     if args.case:
         run_case(args.case)
         return
