@@ -755,6 +755,9 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_row
   constexpr int N = 1 << LOGN, NP = P::len(N);
   constexpr int logN = LOGN;
   constexpr int RB = rows_per_block(LOGN);
+  // the bank's levels in one launch: level blockIdx.y's weights and spectrum, both consecutive
+  if (WEIGHT) wt += (size_t)blockIdx.y * (2 * N) * h;
+  half += (size_t)blockIdx.y * h * N;
   const int row0 = blockIdx.x * RB;
   const int tid = threadIdx.x;
   // load rows as complex pairs (v[2n], v[2n+1]): one 2-wide vector load per pair. The block has
@@ -854,6 +857,9 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS, sizeof(T) == 4 ? 2 : 1) k_col
   constexpr int HP = col_pitch(h);
   constexpr int CPB = cols_per_block(LOGH, (int)sizeof(C));
   constexpr int logc = CPB == 1 ? 0 : CPB == 2 ? 1 : CPB == 4 ? 2 : CPB == 8 ? 3 : CPB == 16 ? 4 : CPB == 32 ? 5 : CPB == 64 ? 6 : CPB == 128 ? 7 : 8;
+  // the bank's levels in one launch: level + blockIdx.y, its spectrum consecutive
+  half += (size_t)blockIdx.y * h * N;
+  level += blockIdx.y;
   const int k0 = blockIdx.x * CPB;
   const int tid = threadIdx.x;
   const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
@@ -1047,6 +1053,15 @@ __device__ __forceinline__ C rot_pi(int e) {
 __host__ __device__ constexpr int cols_per_block_fused(int logh, int elem) {
   return cols_per_block(logh, elem) > 1 ? cols_per_block(logh, elem) / 2 : 1;
 }
+// Column pitch of the fused pass: the padded length rounded up to 16 / CPB (mod 16). Its first
+// stage and the first stage's adjoint have a half warp touch 16 / CPB consecutive butterflies of
+// each of CPB columns, slots cc pitch + j + r (mod 16) in 8-byte units, which are then 16
+// distinct slots (two columns at a pitch of 4 (mod 16), k_cols's, would overlap in 4 of them).
+__host__ __device__ constexpr int col_pitch_fused(int h, int cpb) {
+  int l = h + (h >> 4) + 1;
+  int want = cpb >= 16 ? 1 : 16 / cpb;
+  return l + ((want - l % 16) % 16 + 16) % 16;
+}
 
 template <class T, int LOGH>
 __global__ void __launch_bounds__(FFT_MAX_THREADS / 2, 3) k_cols_fused(int N, cplx<T>* __restrict__ half, const cplx<T>* __restrict__ tw,
@@ -1059,8 +1074,8 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS / 2, 3) k_cols_fused(int N, cp
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   constexpr int h = 1 << LOGH;
-  constexpr int HP = col_pitch(h);
   constexpr int CPB = cols_per_block_fused(LOGH, (int)sizeof(C));
+  constexpr int HP = col_pitch_fused(h, CPB);
   constexpr int logc = CPB == 1 ? 0 : CPB == 2 ? 1 : CPB == 4 ? 2 : CPB == 8 ? 3 : CPB == 16 ? 4 : 5;
   constexpr int NT = CPB * h / FFT_EPT;
   constexpr int RL = last_radix(LOGH);
@@ -1070,6 +1085,9 @@ __global__ void __launch_bounds__(FFT_MAX_THREADS / 2, 3) k_cols_fused(int N, cp
   constexpr int TPC = h / FFT_EPT;    // threads a column
   static_assert(RL < 16 && LOGH >= 5 && B >= 2 && NS % 16 == 0, "the fused column pass: a last radix below 16");
   static_assert(TPC * CPB == NT, "columns: whole threads");
+  // the bank's levels in one launch: level + blockIdx.y, its spectrum consecutive
+  half += (size_t)blockIdx.y * h * N;
+  level += blockIdx.y;
   const int k0 = blockIdx.x * CPB;
   const int tid = threadIdx.x;
   const T dref = (T)S->node_d[level], cref = (T)S->c_ref;
@@ -2029,6 +2047,10 @@ struct dt_flex {
   // the bank's inverse row pass as the persistent, bulk-copy-fed k_rows_inv_bank where the row
   // length allows; DT_ROWS_BANK=0 at create keeps k_rows_inv (the same values, for comparison)
   bool rows_bank = true;
+  // the bank's three forward row passes in one launch and its three column passes in another
+  // (blockIdx.y the level) where the transforms are the power-of-two kernels; DT_BANK_ONE_LAUNCH=0
+  // at create runs each level's two passes as a branch of its own (the same values, for comparison)
+  bool bank_one_launch = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   int sms = 148;
   // the TMA stencil: on when the raster's rows are whole tiles; its tensor maps, one per buffer
@@ -2419,11 +2441,11 @@ static FftGeo fft_geometry(const dt_flex* s) {
   g.rgrid = ceil_div(s->h, RB);
   g.rthreads = std::max(1, RB * N / FFT_EPT);
   g.rsmem = (size_t)RB * Pad<C>::len(N) * sizeof(C);
-  int cpb = s->cols_fused && cols_fusable<T>(logh) ? cols_per_block_fused(logh, (int)sizeof(C))
-                                                   : cols_per_block(logh, (int)sizeof(C));
+  const bool fused = s->cols_fused && cols_fusable<T>(logh);
+  int cpb = fused ? cols_per_block_fused(logh, (int)sizeof(C)) : cols_per_block(logh, (int)sizeof(C));
   g.cgrid = ceil_div(N, cpb);
   g.cthreads = std::max(1, cpb * s->h / FFT_EPT);
-  g.csmem = (size_t)cpb * col_pitch(s->h) * sizeof(C);
+  g.csmem = (size_t)cpb * (fused ? col_pitch_fused(s->h, cpb) : col_pitch(s->h)) * sizeof(C);
   return g;
 }
 
@@ -2692,8 +2714,22 @@ static void launch_precondition(dt_flex* s, Lane<T>& L, const T* r, T* z, int le
   }
   launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, r, L.left, L.S, st);  // left = r - A(J r)
   // part = sum_k w_k S_k(w_k left): the three levels' forward transforms and column passes are
-  // independent, so levels 1 and 2 run on side streams (parallel branches when captured into the
-  // loop graph); one inverse pass then takes the three spectra to the weighted sum
+  // independent. With the power-of-two kernels each pass takes the three levels in one launch
+  // (their spectra and weights are consecutive); otherwise levels 1 and 2 run on side streams
+  // (parallel branches when captured into the loop graph). One inverse pass then takes the
+  // three spectra to the weighted sum.
+  if (s->bank_one_launch && !s->any && !s->row_solve) {
+    FftGeo g = fft_geometry<T>(s);
+    rows_fwd_fn<T, true>(ilog2(s->N), LogSeq{})<<<dim3(g.rgrid, 3), g.rthreads, g.rsmem, st>>>(
+        s->w, s->h, L.left, L.wt[0], L.half, L.tab.tw_row, L.tab.post, L.S);
+    counted();
+    cols_fn<T>(ilog2(s->h), LogSeq{}, s->cols_fused)<<<dim3(g.cgrid, 3), g.cthreads, g.csmem, st>>>(
+        s->N, L.half, L.tab.tw_col, L.tab.omega, L.tab.omega2, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), L.S, 0);
+    counted();
+    launch_rows_inv<T>(s, L, INV_BANK, L.half, L.part, L.wt[0], nullptr, g, L.S, st);
+    launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, r, z, L.S, st);  // z = u + J(r - A u)
+    return;
+  }
   cudaEventRecord(s->ev_fork, st);
   cudaStreamWaitEvent(s->side[0], s->ev_fork, 0);
   cudaStreamWaitEvent(s->side[1], s->ev_fork, 0);
@@ -3340,6 +3376,7 @@ dt_status dt_flex_create(int w, int h, double dx, const double* metric_a, const 
   if (const char* e = getenv("DT_STENCIL_WAIT_GIVE_UP")) s->wait_give_up = e[0] == '1';
   if (const char* e = getenv("DT_COLS_FUSED")) s->cols_fused = e[0] != '0';
   if (const char* e = getenv("DT_ROWS_BANK")) s->rows_bank = e[0] != '0';
+  if (const char* e = getenv("DT_BANK_ONE_LAUNCH")) s->bank_one_launch = e[0] != '0';
 
   // RowMetric::block (flexure.rs:1000-1010): the block metric's couplings, for a height the
   // cosine transform does not take
