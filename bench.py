@@ -786,6 +786,22 @@ def diffusion_leg(lib, stream, timed, max_over_ranks, world, steps, check=True):
             got = x_dev.cpu().numpy()
             out[name]["rel_l2"] = float(np.linalg.norm(got - exact) / np.linalg.norm(exact))
             out[name]["max_abs_m"] = float(np.abs(got - exact).max())
+    # the finest level's hot kernels, each launch alone after an L2 flush: bandwidth over their
+    # algorithmic bytes, against the measured copy peak
+    peaks = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak = json.load(open(peaks))["hbm_gbs"] if os.path.exists(peaks) else 6650.0
+    def kernels(prof):
+        return {name: {"ms": t, "algorithmic_bytes": by, "GB/s": by / (t * 1e-3) / 1e9,
+                       "frac_of_hbm_peak": by / (t * 1e-3) / 1e9 / peak} for name, (t, by) in prof.items()}
+
+    out["kernels"] = kernels(ws.profile_kernels(sets[0][1] * dx * dx / dt, dt))
+    # the same kernels at 8192 x 4096, where a launch is long enough that its fixed costs (the
+    # ramp of the grid, the last block's reduction) weigh little beside its bytes
+    wl, hl = 8192, 4096
+    big = D.Workspace(D.Dims(wl, hl, dx, True))
+    _, sl = I.diffusion_problem(wl, hl, 8.0, 3000)
+    out["kernels_8192x4096"] = kernels(big.profile_kernels(sl * dx * dx / dt, dt))
+    big.close()
     out["speedup_mixed_vs_fp64"] = out["fp64_rbgs"]["ms_per_solve"] / out["mixed_rbgs"]["ms_per_solve"]
     out["speedup_mixed_reliable_vs_fp64"] = out["fp64_rbgs"]["ms_per_solve"] / out["mixed_reliable_rbgs"]["ms_per_solve"]
     ws.close()

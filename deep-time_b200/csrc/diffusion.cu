@@ -114,6 +114,64 @@ __device__ __forceinline__ T d_apply_at(int w, int h, bool wrap, const T* __rest
 
 enum { DA_PAP = 0, DA_RESID = 1, DA_MASS = 2, DA_PLAIN = 3, DA_RESID_GATED = 4 };
 
+// 16 bytes of T, for whole-word loads and stores of a row chunk
+template <class T>
+struct alignas(16) DV16 {
+  T a[16 / sizeof(T)];
+};
+__device__ __forceinline__ bool d_aligned16(const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+// y = A x on the row chunk of V = 16 / sizeof(T) cells i0 .. i0 + V - 1 of row j (V divides w),
+// every cell's terms in d_apply_at's order: 16-byte loads of the chunk's diag, east and x and of
+// the rows below and above (south, x), one value each for the neighbours across the chunk's ends
+// (the row's other end where x wraps). 32-bit offsets: the raster has fewer than 2^31 cells.
+template <class T>
+__device__ __forceinline__ void d_apply_chunk(int w, int h, bool wrap, const T* __restrict__ east, const T* __restrict__ south,
+                                              const T* __restrict__ diag, const T* __restrict__ x, int i0, int j,
+                                              DV16<T>& ax, DV16<T>& xv, DV16<T>& dg) {
+  constexpr int V = 16 / sizeof(T);
+  using W = DV16<T>;
+  const int c0 = j * w, c = c0 + i0;
+  dg = *reinterpret_cast<const W*>(diag + c);
+  xv = *reinterpret_cast<const W*>(x + c);
+  const W ea = *reinterpret_cast<const W*>(east + c);
+  T xl = (T)0, el = (T)0, xr = (T)0;
+  if (i0 > 0) {
+    xl = x[c - 1];
+    el = east[c - 1];
+  } else if (wrap) {
+    xl = x[c0 + w - 1];
+    el = east[c0 + w - 1];
+  }
+  if (i0 + V < w)
+    xr = x[c + V];
+  else if (wrap)
+    xr = x[c0];
+  W xs = {}, ss = {}, xn = {}, sn = {};
+  if (j + 1 < h) {
+    xs = *reinterpret_cast<const W*>(x + c + w);
+    ss = *reinterpret_cast<const W*>(south + c);
+  }
+  if (j > 0) {
+    xn = *reinterpret_cast<const W*>(x + c - w);
+    sn = *reinterpret_cast<const W*>(south + c - w);
+  }
+#pragma unroll
+  for (int e = 0; e < V; ++e) {
+    const int i = i0 + e;
+    const T xe = e + 1 < V ? xv.a[e + 1] : xr;  // east neighbour; x[c0] across the seam
+    const T xw = e > 0 ? xv.a[e - 1] : xl, ew = e > 0 ? ea.a[e - 1] : el;  // west neighbour and its east face
+    T o = dg.a[e] * xv.a[e];
+    if (i + 1 < w) o -= ea.a[e] * xe;
+    if (wrap && i == w - 1) o -= ea.a[e] * xe;
+    if (i > 0) o -= ew * xw;
+    if (wrap && i == 0) o -= ew * xw;
+    if (j + 1 < h) o -= ss.a[e] * xs.a[e];
+    if (j > 0) o -= sn.a[e] * xn.a[e];
+    ax.a[e] = o;
+  }
+}
+
 // DA_PAP: y = A x, reduce x.y; DA_RESID: y = b - A x, ym = (TM) y, reduce y.y;
 // DA_MASS: reduce sum (b - A x) and sum (diag - 1); DA_PLAIN: y = A x; DA_RESID_GATED: in an
 // iteration that replaces the residual (S->gate_it == S->it), y = b - A x and y.y -> S->rr_true.
@@ -130,26 +188,66 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
   Acc<2> acc;
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(k % w), j = (int)(k / w);
-    T ax = d_apply_at<T>(w, h, wrap != 0, east, south, diag, x, i, j);
-    if (MODE == DA_PAP) {
-      y[k] = ax;
-      acc.v[0] += (double)x[k] * (double)ax;
-    } else if (MODE == DA_RESID) {
-      T r = b[k] - ax;
-      y[k] = r;
-      ym[k] = (TM)r;
-      acc.v[0] += (double)r * (double)r;
-    } else if (MODE == DA_RESID_GATED) {
-      T r = b[k] - ax;
-      y[k] = r;
-      acc.v[0] += (double)r * (double)r;
-    } else if (MODE == DA_MASS) {
-      acc.v[0] += (double)b[k] - (double)ax;
-      acc.v[1] += (double)diag[k] - 1.0;
-    } else {
-      y[k] = ax;
+  constexpr int V = 16 / sizeof(T);
+  if (w % V == 0 && d_aligned16(east) && d_aligned16(south) && d_aligned16(diag) && d_aligned16(x) && d_aligned16(b) &&
+      d_aligned16(y)) {
+    // whole rows of 16-byte chunks: each thread a chunk at a time
+    const unsigned int chunks = (unsigned int)(w / V), nch = chunks * (unsigned int)h;
+    for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < nch; q += gridDim.x * blockDim.x) {
+      const int j = (int)(q / chunks), i0 = (int)(q - (unsigned int)j * chunks) * V;
+      const int c = j * w + i0;
+      DV16<T> ax, xv, dg;
+      d_apply_chunk<T>(w, h, wrap != 0, east, south, diag, x, i0, j, ax, xv, dg);
+      DV16<T> bv = {};
+      if (MODE == DA_RESID || MODE == DA_RESID_GATED || MODE == DA_MASS) bv = *reinterpret_cast<const DV16<T>*>(b + c);
+      DV16<T> out;
+#pragma unroll
+      for (int e = 0; e < V; ++e) {
+        const T a = ax.a[e];
+        if (MODE == DA_PAP) {
+          out.a[e] = a;
+          acc.v[0] += (double)xv.a[e] * (double)a;
+        } else if (MODE == DA_RESID) {
+          const T r = bv.a[e] - a;
+          out.a[e] = r;
+          ym[c + e] = (TM)r;
+          acc.v[0] += (double)r * (double)r;
+        } else if (MODE == DA_RESID_GATED) {
+          const T r = bv.a[e] - a;
+          out.a[e] = r;
+          acc.v[0] += (double)r * (double)r;
+        } else if (MODE == DA_MASS) {
+          acc.v[0] += (double)bv.a[e] - (double)a;
+          acc.v[1] += (double)dg.a[e] - 1.0;
+        } else {
+          out.a[e] = a;
+        }
+      }
+      if (MODE != DA_MASS) *reinterpret_cast<DV16<T>*>(y + c) = out;
+    }
+  } else {
+    // other widths and unaligned arrays: one cell at a time
+    for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
+      int i = (int)(k % w), j = (int)(k / w);
+      T ax = d_apply_at<T>(w, h, wrap != 0, east, south, diag, x, i, j);
+      if (MODE == DA_PAP) {
+        y[k] = ax;
+        acc.v[0] += (double)x[k] * (double)ax;
+      } else if (MODE == DA_RESID) {
+        T r = b[k] - ax;
+        y[k] = r;
+        ym[k] = (TM)r;
+        acc.v[0] += (double)r * (double)r;
+      } else if (MODE == DA_RESID_GATED) {
+        T r = b[k] - ax;
+        y[k] = r;
+        acc.v[0] += (double)r * (double)r;
+      } else if (MODE == DA_MASS) {
+        acc.v[0] += (double)b[k] - (double)ax;
+        acc.v[1] += (double)diag[k] - 1.0;
+      } else {
+        y[k] = ax;
+      }
     }
   }
   if (MODE == DA_PLAIN) return;
@@ -611,54 +709,95 @@ __global__ void __launch_bounds__(1024) k_mg_coarse_rb(MgChain<TM> g, int nu, in
 }
 
 // Two red-black Gauss-Seidel sweeps (four colour passes) of a level in one launch, over tiles of
-// MG_TX x MG_TY cells staged in shared memory with a halo: pass p updates its colour on the tile
-// and the rings around it that the later passes read, so the tile's cells end with the values
-// four separate passes give (temporal blocking; each update is gs_cell's, term for term).
-//   PRE   the pre-smoothing: z from 0, colours 0, 1, 0, 1; then the residual r - A z on the
-//         tile and its 2 x 2 sums into the coarser level's r (k_mg_restrict's arithmetic), so
-//         the restriction needs no launch of its own (halo 5: z is final one ring out);
+// TX x TY cells staged in shared memory with a halo: pass p updates its colour on the tile and
+// the rings around it that the later passes read, so the tile's cells end with the values four
+// separate passes give (temporal blocking; each update is gs_cell's, term for term).
+//   PRE   the pre-smoothing: z from 0, colours 0, 1, 0, 1; then the residual r - A z of each
+//         of the tile's cells (mg_apply_at's order) and its 2 x 2 sums, in k_mg_restrict's
+//         order, into the coarser level's r, so the restriction needs no launch of its own
+//         (halo 5: z is final one ring out);
 //   !PRE  the post-smoothing: z += P zc (the coarse correction, piecewise constant), then
 //         colours 1, 0, 1, 0 (halo 4). It reads z around its tile, which neighbouring tiles
 //         finish at the same time, so it writes its result to another buffer (zout = L.t; PRE,
 //         which reads no z, writes L.z).
-// For levels of two colours (no wrap, or an even width) at least MG_TX + 10 cells wide, so that
-// no cell sits twice in a tile. Shared memory holds the region in red-black order, so that a
-// colour pass reads and writes consecutive words with no idle lanes.
-constexpr int MG_TX = 32, MG_TY = 16;
-template <class TM, bool PRE>
-__global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, const TM* __restrict__ zc, TM* __restrict__ zout) {
+// For levels of two colours (no wrap, or an even width) at least TX + 10 cells wide, so that no
+// cell sits twice in a tile, and of fewer than 2^31 cells (32-bit offsets). Shared memory holds
+// the region in red-black order, so that a colour pass reads and writes consecutive words with
+// no idle lanes. A tile whose region lies inside the raster (most tiles) stages and updates
+// without the bounds and seam tests, whose outcome is known there: every neighbour exists and
+// none lies across the seam.
+// Tiles: 32 x 16 cells and 256 threads; FP32 levels of many tiles take 64 x 32 cells and 512
+// threads, which cuts the halo's staged cells per tile cell from 2.1 to 1.5 and its updates
+// from 3.1 to 2.5.
+constexpr int MG_TX = 32, MG_TY = 16, MG_BTX = 64, MG_BTY = 32;
+// One value from global into shared memory by an asynchronous copy (completes at the block's
+// cp.async.wait_all).
+__device__ __forceinline__ void rb2_cp_async(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void rb2_cp_async(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src) : "memory");
+}
+template <class TM, bool PRE, int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, const TM* __restrict__ zc, TM* __restrict__ zout) {
   constexpr int HALO = PRE ? 5 : 4;
-  constexpr int SX = MG_TX + 2 * HALO, SY = MG_TY + 2 * HALO;
+  constexpr int SX = TX + 2 * HALO, SY = TY + 2 * HALO;
   constexpr int HX = SX / 2, NC = HX * SY;  // a colour's cells of a row, of the region
-  static_assert(SX % 2 == 0, "rb2: even rows");
+  static_assert(SX % 2 == 0 && 2 * NC >= TX * TY, "rb2: even rows");
   // red-black layout: cell (lx, ly) of colour k = (i0 + lx + j0 + ly) & 1 at a[k][ly * HX + lx / 2]
   extern __shared__ __align__(16) unsigned char mg_smem[];
   TM* const base = reinterpret_cast<TM*>(mg_smem);
   // array a (0 z, 1 r, 2 diag, 3 wd, 4 east, 5 south) of colour k
   auto A = [&](int a, int k) { return base + (2 * a + k) * NC; };
-  const int i0 = blockIdx.x * MG_TX - HALO, j0 = blockIdx.y * MG_TY - HALO;
+  const int i0 = blockIdx.x * TX - HALO, j0 = blockIdx.y * TY - HALO;
   const int off = (i0 + j0) & 1;
   const int tid = threadIdx.x;
   const int w = L.w, h = L.h;
+  const bool inner = i0 >= 0 && j0 >= 0 && i0 + SX <= w && j0 + SY <= h;
   auto gcol = [&](int lx) {
     int gi = i0 + lx;
     if (L.wrap) gi = gi < 0 ? gi + w : (gi >= w ? gi - w : gi);
     return gi;
   };
-  for (int e = tid; e < SX * SY; e += 256) {
-    const int ly = e / SX, lx = e - ly * SX;
-    const int gi = gcol(lx), gj = j0 + ly;
-    if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
+  // staging by asynchronous copies into the colour arrays, so that all of a thread's copies are
+  // in flight at once (a load into registers and a store per value would wait out each load
+  // in turn); the post-smoothing then adds the coarse correction to its own staged z values
+  auto stage = [&](int lx, int ly, int gi, int gj) {
     const int k = (lx + ly + off) & 1, q = ly * HX + (lx >> 1);
-    const size_t c = (size_t)gj * w + gi;
-    TM zv = PRE ? (TM)0 : L.z[c];
-    if (!PRE) zv += zc[(size_t)(gj / 2) * C.w + gi / 2];
-    A(0, k)[q] = zv;
-    A(1, k)[q] = L.r[c];
-    A(2, k)[q] = L.diag[c];
-    A(3, k)[q] = L.wd[c];
-    A(4, k)[q] = L.east[c];
-    A(5, k)[q] = L.south[c];
+    const int c = gj * w + gi;
+    if (PRE)
+      A(0, k)[q] = (TM)0;
+    else
+      rb2_cp_async(A(0, k) + q, L.z + c);
+    rb2_cp_async(A(1, k) + q, L.r + c);
+    rb2_cp_async(A(2, k) + q, L.diag + c);
+    rb2_cp_async(A(3, k) + q, L.wd + c);
+    rb2_cp_async(A(4, k) + q, L.east + c);
+    rb2_cp_async(A(5, k) + q, L.south + c);
+  };
+  if (inner) {
+    for (int e = tid; e < SX * SY; e += NT) {
+      const int ly = e / SX, lx = e - ly * SX;
+      stage(lx, ly, i0 + lx, j0 + ly);
+    }
+  } else {
+    for (int e = tid; e < SX * SY; e += NT) {
+      const int ly = e / SX, lx = e - ly * SX;
+      const int gi = gcol(lx), gj = j0 + ly;
+      if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
+      stage(lx, ly, gi, gj);
+    }
+  }
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+  if (!PRE) {
+    // z = z + zc (P zc piecewise constant), each thread on the cells it staged
+#pragma unroll 4
+    for (int e = tid; e < SX * SY; e += NT) {
+      const int ly = e / SX, lx = e - ly * SX;
+      const int gi = inner ? i0 + lx : gcol(lx), gj = j0 + ly;
+      if (!inner && (gj < 0 || gj >= h || gi < 0 || gi >= w)) continue;
+      A(0, (lx + ly + off) & 1)[ly * HX + (lx >> 1)] += zc[(gj >> 1) * C.w + (gi >> 1)];
+    }
   }
   __syncthreads();
   // pass p updates its colour at least p + 1 cells from the region's border: a row's cells of
@@ -667,67 +806,79 @@ __global__ void __launch_bounds__(256) k_mg_rb2(DLevel<TM> L, DLevel<TM> C, cons
   for (int pass = 0; pass < 4; ++pass) {
     const int k = PRE ? (pass & 1) : 1 - (pass & 1), o_ = 1 - k;
     const int lo = pass + 1, RW = SX - 2 * lo, RH = SY - 2 * lo, HW = RW / 2;
-    const TM* zo = A(0, o_);
-    for (int idx = tid; idx < RH * HW; idx += 256) {
+    TM* const zs = A(0, k);
+    const TM* const zo = A(0, o_);
+    const TM *const rk = A(1, k), *const dk = A(2, k), *const wk = A(3, k);
+    const TM *const ek = A(4, k), *const eo = A(4, o_), *const sk = A(5, k), *const so = A(5, o_);
+    for (int idx = tid; idx < RH * HW; idx += NT) {
       const int ly = lo + idx / HW;
       const int p = (k + ly + off) & 1;  // the parity of lx of colour k on this row
       const int lx = lo + ((p - lo) & 1) + 2 * (idx - (ly - lo) * HW);
-      const int gi = gcol(lx), gj = j0 + ly;
-      if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
       const int q = ly * HX + (lx >> 1);
       const int qw = ly * HX + ((lx - 1) >> 1), qe = ly * HX + ((lx + 1) >> 1);  // the other colour's
-      TM* const zs = A(0, k);
       const TM zk = zs[q];
-      const TM ec = A(4, k)[q], ew = A(4, o_)[qw];
-      TM o = mulr(A(2, k)[q], zk);
-      if (gi + 1 < w) o -= mulr(ec, zo[qe]);
-      if (gi > 0) o -= mulr(ew, zo[qw]);
-      if (L.wrap) {
-        if (gi == w - 1) o -= mulr(ec, zo[qe]);
-        if (gi == 0) o -= mulr(ew, zo[qw]);
+      TM o = mulr(dk[q], zk);
+      if (inner) {
+        o -= mulr(ek[q], zo[qe]);
+        o -= mulr(eo[qw], zo[qw]);
+        o -= mulr(sk[q], zo[q + HX]);
+        o -= mulr(so[q - HX], zo[q - HX]);
+      } else {
+        const int gi = gcol(lx), gj = j0 + ly;
+        if (gj < 0 || gj >= h || gi < 0 || gi >= w) continue;
+        if (gi + 1 < w) o -= mulr(ek[q], zo[qe]);
+        if (gi > 0) o -= mulr(eo[qw], zo[qw]);
+        if (L.wrap) {
+          if (gi == w - 1) o -= mulr(ek[q], zo[qe]);
+          if (gi == 0) o -= mulr(eo[qw], zo[qw]);
+        }
+        if (gj + 1 < h) o -= mulr(sk[q], zo[q + HX]);
+        if (gj > 0) o -= mulr(so[q - HX], zo[q - HX]);
       }
-      if (gj + 1 < h) o -= mulr(A(5, k)[q], zo[q + HX]);
-      if (gj > 0) o -= mulr(A(5, o_)[q - HX], zo[q - HX]);
-      zs[q] = zk + mulr(A(1, k)[q] - o, A(3, k)[q]);
+      zs[q] = zk + mulr(rk[q] - o, wk[q]);
     }
     __syncthreads();
   }
   auto at = [&](int a, int lx, int ly) -> TM { return A(a, (lx + ly + off) & 1)[ly * HX + (lx >> 1)]; };
   if (PRE) {
-    // the residual of the tile's cells (mg_apply_at's order) summed over 2 x 2 blocks into C.r,
-    // in k_mg_restrict's order
-    constexpr int CX = MG_TX / 2, CY = MG_TY / 2;
-    if (tid < CX * CY) {
-      const int ic = blockIdx.x * CX + tid % CX, jc = blockIdx.y * CY + tid / CX;
-      if (ic < C.w && jc < C.h) {
-        TM acc = 0;
-        for (int j = 2 * jc; j < min(2 * jc + 2, h); ++j)
-          for (int i = 2 * ic; i < min(2 * ic + 2, w); ++i) {
-            const int lx = i - i0, ly = j - j0;
-            TM o = mulr(at(2, lx, ly), at(0, lx, ly));
-            if (i + 1 < w) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
-            if (i > 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
-            if (L.wrap) {
-              if (i == w - 1) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
-              if (i == 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
-            }
-            if (j + 1 < h) o -= mulr(at(5, lx, ly), at(0, lx, ly + 1));
-            if (j > 0) o -= mulr(at(5, lx, ly - 1), at(0, lx, ly - 1));
-            acc += at(1, lx, ly) - o;
-          }
-        C.r[(size_t)jc * C.w + ic] = acc;
+    // the residual of each of the tile's cells, in mg_apply_at's order, into the slots of 1/diag
+    // (no longer read); then each coarse cell's 2 x 2 sum in k_mg_restrict's order
+    TM* const res = A(3, 0);
+    for (int e = tid; e < TX * TY; e += NT) {
+      const int lx = HALO + e % TX, ly = HALO + e / TX;
+      const int i = i0 + lx, j = j0 + ly;
+      if (i >= w || j >= h) continue;
+      TM o = mulr(at(2, lx, ly), at(0, lx, ly));
+      if (i + 1 < w) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
+      if (i > 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
+      if (L.wrap) {
+        if (i == w - 1) o -= mulr(at(4, lx, ly), at(0, lx + 1, ly));
+        if (i == 0) o -= mulr(at(4, lx - 1, ly), at(0, lx - 1, ly));
       }
+      if (j + 1 < h) o -= mulr(at(5, lx, ly), at(0, lx, ly + 1));
+      if (j > 0) o -= mulr(at(5, lx, ly - 1), at(0, lx, ly - 1));
+      res[e] = at(1, lx, ly) - o;
+    }
+    __syncthreads();
+    constexpr int CX = TX / 2, CY = TY / 2;
+    for (int t = tid; t < CX * CY; t += NT) {
+      const int ic = blockIdx.x * CX + t % CX, jc = blockIdx.y * CY + t / CX;
+      if (ic >= C.w || jc >= C.h) continue;
+      TM acc = 0;
+      for (int j = 2 * jc; j < min(2 * jc + 2, h); ++j)
+        for (int i = 2 * ic; i < min(2 * ic + 2, w); ++i) acc += res[(j - j0 - HALO) * TX + (i - i0 - HALO)];
+      C.r[jc * C.w + ic] = acc;
     }
   }
-  for (int e = tid; e < MG_TX * MG_TY; e += 256) {
-    const int ly = HALO + e / MG_TX, lx = HALO + e % MG_TX;
+  for (int e = tid; e < TX * TY; e += NT) {
+    const int ly = HALO + e / TX, lx = HALO + e % TX;
     const int gi = i0 + lx, gj = j0 + ly;
-    if (gi < w && gj < h) zout[(size_t)gj * w + gi] = at(0, lx, ly);
+    if (gi < w && gj < h) zout[gj * w + gi] = at(0, lx, ly);
   }
 }
-template <class TM, bool PRE>
+template <class TM, bool PRE, int TX = MG_TX, int TY = MG_TY>
 constexpr size_t mg_rb2_smem() {
-  return (size_t)6 * (MG_TX + 2 * (PRE ? 5 : 4)) * (MG_TY + 2 * (PRE ? 5 : 4)) * sizeof(TM);
+  return (size_t)6 * (TX + 2 * (PRE ? 5 : 4)) * (TY + 2 * (PRE ? 5 : 4)) * sizeof(TM);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1002,6 +1153,11 @@ __global__ void k_d_arm(DScalars* S, unsigned long long handle, unsigned long lo
   S->body_runs = 0;
   cudaGraphSetConditional((cudaGraphConditionalHandle)handle, S->stop == 0 ? 1u : 0u);
 }
+// dt_diff_profile_kernels: a solve's state record ready for one more operator launch
+__global__ void k_d_profile_state(DScalars* S) {
+  S->stop = 0;
+  S->cond = 0ull;
+}
 __global__ void k_d_disarm(DScalars* S) {
   S->cond = 0ull;
   S->cond_if = 0ull;
@@ -1175,9 +1331,25 @@ struct dt_diff {
   // the Gauss-Seidel cycle's fused kernels (k_mg_rb2, k_mg_coarse_rb); DT_MG_FUSED=0 at create
   // keeps one launch per colour pass (the same values)
   bool mg_fused = true;
+  // k_mg_rb2's 64 x 32 tiles on FP32 levels of many tiles; DT_MG_BIG_TILES=0 at create keeps
+  // 32 x 16 tiles everywhere (the same values)
+  bool mg_big_tiles = true;
 };
 
 namespace dt {
+
+// Opt k_mg_rb2's instantiations in to their dynamic shared memory.
+template <class TM>
+static void rb2_attributes() {
+  cudaFuncSetAttribute(k_mg_rb2<TM, true, MG_TX, MG_TY, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mg_rb2_smem<TM, true>());
+  cudaFuncSetAttribute(k_mg_rb2<TM, false, MG_TX, MG_TY, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mg_rb2_smem<TM, false>());
+  cudaFuncSetAttribute(k_mg_rb2<TM, true, MG_BTX, MG_BTY, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mg_rb2_smem<TM, true, MG_BTX, MG_BTY>());
+  cudaFuncSetAttribute(k_mg_rb2<TM, false, MG_BTX, MG_BTY, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)mg_rb2_smem<TM, false, MG_BTX, MG_BTY>());
+}
 
 template <class T>
 static dt_status ddalloc(dt_diff* s, T** p, size_t count) {
@@ -1242,6 +1414,28 @@ static void fill_levels(dt_diff* s, Hier<TM>& H, int kind, cudaStream_t st) {
   }
 }
 
+// Whether k_mg_rb2 takes a level: at least MG_TX + 10 cells wide (no cell twice in a tile's
+// region) and fewer than 2^31 cells (its 32-bit offsets).
+template <class TM>
+static bool rb2_fits(const DLevel<TM>& L) {
+  return L.w >= MG_TX + 10 && (size_t)L.w * L.h < ((size_t)1 << 31);
+}
+// The two tiled sweeps of a level (PRE: from z = 0 with the restriction into C.r; else with the
+// coarse correction zc): 64 x 32 tiles for FP32 levels of at least four tiles an SM, else 32 x 16.
+template <class TM, bool PRE>
+static void launch_rb2(dt_diff* s, const DLevel<TM>& L, const DLevel<TM>& C, const TM* zc, TM* zout, cudaStream_t st) {
+  const bool big = std::is_same<TM, float>::value && s->mg_big_tiles && L.w >= MG_BTX + 10 &&
+                   (size_t)ceil_div(L.w, MG_BTX) * ceil_div(L.h, MG_BTY) >= (size_t)4 * s->sms;
+  if (big) {
+    const dim3 tg(ceil_div(L.w, MG_BTX), ceil_div(L.h, MG_BTY));
+    k_mg_rb2<TM, PRE, MG_BTX, MG_BTY, 512><<<tg, 512, mg_rb2_smem<TM, PRE, MG_BTX, MG_BTY>(), st>>>(L, C, zc, zout);
+  } else {
+    const dim3 tg(ceil_div(L.w, MG_TX), ceil_div(L.h, MG_TY));
+    k_mg_rb2<TM, PRE, MG_TX, MG_TY, 256><<<tg, 256, mg_rb2_smem<TM, PRE>(), st>>>(L, C, zc, zout);
+  }
+  count_launch();
+}
+
 // One V-cycle from z = 0 on level l with r set; returns the buffer holding the level's z.
 template <class TM>
 static TM* vcycle(dt_diff* s, Hier<TM>& H, size_t l, int kind, cudaStream_t st) {
@@ -1304,13 +1498,10 @@ static TM* vcycle(dt_diff* s, Hier<TM>& H, size_t l, int kind, cudaStream_t st) 
     }
     // both sweeps of the smoothing in one launch over tiles, the restriction fused into the
     // pre-smoothing (two-colour levels wide enough)
-    if (ncol == 2 && NU == 2 && L.w >= MG_TX + 10) {
-      const dim3 tg(ceil_div(L.w, MG_TX), ceil_div(L.h, MG_TY));
-      k_mg_rb2<TM, true><<<tg, 256, mg_rb2_smem<TM, true>(), st>>>(L, C, nullptr, L.z);
-      count_launch();
+    if (ncol == 2 && NU == 2 && rb2_fits(L)) {
+      launch_rb2<TM, true>(s, L, C, nullptr, L.z, st);
       TM* zc = vcycle<TM>(s, H, l + 1, kind, st);
-      k_mg_rb2<TM, false><<<tg, 256, mg_rb2_smem<TM, false>(), st>>>(L, C, zc, L.t);
-      count_launch();
+      launch_rb2<TM, false>(s, L, C, zc, L.t, st);
       return L.t;  // the level's z, in its spare buffer
     }
   }
@@ -1751,10 +1942,9 @@ dt_status dt_diff_create(int w, int h, double dx, int wrap_x, dt_diff** out) {
   // rounding up) in six arrays
   cudaFuncSetAttribute(k_mg_coarse_rb<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   cudaFuncSetAttribute(k_mg_coarse_rb<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(k_mg_rb2<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<float, true>());
-  cudaFuncSetAttribute(k_mg_rb2<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<float, false>());
-  cudaFuncSetAttribute(k_mg_rb2<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<double, true>());
-  cudaFuncSetAttribute(k_mg_rb2<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mg_rb2_smem<double, false>());
+  if (const char* e = getenv("DT_MG_BIG_TILES")) s->mg_big_tiles = e[0] != '0';
+  rb2_attributes<float>();
+  rb2_attributes<double>();
   s->n = (size_t)w * h;
   cudaDeviceProp prop;
   if (cudaGetDeviceProperties(&prop, 0) == cudaSuccess) s->sms = prop.multiProcessorCount;
@@ -1973,6 +2163,100 @@ dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, con
   DT_CUDA(cudaStreamSynchronize(st));
   if (levels) *levels = (int)H.lv.size();
   return DT_OK;
+}
+
+// Benchmark support: the CG operator (with p.Ap) and the Gauss-Seidel cycle's two tiled sweep
+// pairs on the finest level, each launch timed alone (CUDA events on the handle's stream) after
+// a write of a buffer twice the L2, so that it reads its inputs from HBM; ms[k] the mean of
+// `reps` launches, bytes[k] the launch's algorithmic bytes (each array read once, each output
+// written once). Inputs: x and the levels' r from kd, the coarse correction zero.
+dt_status dt_diff_profile_kernels(dt_diff* s, const double* kd, double dt, int reps, double* ms, double* bytes) {
+  if (!s || !kd || !ms || !bytes || reps < 1 || !(dt > 0.0)) {
+    set_error("dt_diff_profile_kernels: bad argument");
+    return DT_BAD_ARG;
+  }
+  cudaStream_t st = s->stream;
+  const size_t n = s->n;
+  const int wrap = s->wrap && s->w > 1;
+  DT_CUDA(cudaMemcpyAsync(s->kd, kd, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  k_d_coeffs<<<dgrid(s, n), 256, 0, st>>>(s->w, s->h, wrap, s->kd, dt / (s->dx * s->dx), s->east, s->south, s->diag, s->east32,
+                                          s->south32, s->diag32);
+  Hier<float>& HF = s->hf[DT_CYCLE_RBGS];
+  Hier<double>& HD = s->hd[DT_CYCLE_RBGS];
+  DT_TRY(build_levels<float>(s, HF, COARSEST_GS));
+  DT_TRY(build_levels<double>(s, HD, COARSEST_GS));
+  if (HF.lv.size() < 2 || gs_colours(HF.lv[0].w, HF.lv[0].wrap) != 2 || !rb2_fits(HF.lv[0])) {
+    set_error("dt_diff_profile_kernels: the finest level of a %d x %d raster does not take the tiled sweeps", s->w, s->h);
+    return DT_UNSUPPORTED;
+  }
+  fill_levels<float>(s, HF, DT_CYCLE_RBGS, st);
+  fill_levels<double>(s, HD, DT_CYCLE_RBGS, st);
+  DT_CUDA(cudaMemcpyAsync(s->p, s->kd, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  k_convert_dr<<<dgrid(s, n), 256, 0, st>>>(n, s->kd, s->p32);
+  k_convert_dr<<<dgrid(s, n), 256, 0, st>>>(n, s->kd, HF.lv[0].r);
+  DT_CUDA(cudaMemcpyAsync(HD.lv[0].r, s->kd, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  DLevel<float> &F0 = HF.lv[0], &F1 = HF.lv[1];
+  DLevel<double> &D0 = HD.lv[0], &D1 = HD.lv[1];
+  const size_t nc = (size_t)F1.w * F1.h;
+  DT_CUDA(cudaMemsetAsync(F1.z, 0, nc * sizeof(float), st));
+  DT_CUDA(cudaMemsetAsync(D1.z, 0, nc * sizeof(double), st));
+  const unsigned g = dgrid(s, n);
+  auto one = [&](int k) {
+    switch (k) {
+      case 0:
+        k_d_apply<double, float, DA_PAP><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east, s->south, s->diag, s->p, nullptr, s->ap,
+                                                            nullptr, s->partials, s->S64);
+        break;
+      case 1:
+        k_d_apply<float, float, DA_PAP><<<g, 256, 0, st>>>(s->w, s->h, wrap, s->east32, s->south32, s->diag32, s->p32, nullptr,
+                                                           s->ap32, nullptr, s->partials, s->S32);
+        break;
+      case 2: launch_rb2<float, true>(s, F0, F1, nullptr, F0.z, st); break;
+      case 3: launch_rb2<float, false>(s, F0, F1, F1.z, F0.t, st); break;
+      case 4: launch_rb2<double, true>(s, D0, D1, nullptr, D0.z, st); break;
+      default: launch_rb2<double, false>(s, D0, D1, D1.z, D0.t, st); break;
+    }
+  };
+  // algorithmic bytes: the operator x, east, south, diag in and y out; the pre-smoothing r, diag,
+  // 1/diag, east, south in, z and the coarse r out; the post-smoothing z, the coarse z, r, diag,
+  // 1/diag, east, south in and z out
+  const double nf = (double)n, ncd = (double)nc;
+  const double algo[DT_DIFF_PROFILE_KERNELS] = {40 * nf, 20 * nf, 4 * (6 * nf + ncd), 4 * (7 * nf + ncd),
+                                                8 * (6 * nf + ncd), 8 * (7 * nf + ncd)};
+  const size_t flush_bytes = (size_t)256 << 20;
+  void* flush = nullptr;
+  DT_CUDA(cudaMalloc(&flush, flush_bytes));
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  dt_status rc = DT_OK;
+  for (int k = 0; k < DT_DIFF_PROFILE_KERNELS && rc == DT_OK; ++k) {
+    k_d_profile_state<<<1, 1, 0, st>>>(s->S64);
+    k_d_profile_state<<<1, 1, 0, st>>>(s->S32);
+    one(k);  // warm
+    double total = 0.0;
+    for (int r = 0; r < reps; ++r) {
+      cudaMemsetAsync(flush, r & 0xff, flush_bytes, st);
+      cudaEventRecord(a, st);
+      one(k);
+      cudaEventRecord(b, st);
+      cudaEventSynchronize(b);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, a, b);
+      total += t;
+    }
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("dt_diff_profile_kernels: a launch failed");
+      rc = DT_DEVICE_ERROR;
+    }
+    ms[k] = total / reps;
+    bytes[k] = algo[k];
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamSynchronize(st);
+  cudaFree(flush);
+  return rc;
 }
 
 }  // extern "C"

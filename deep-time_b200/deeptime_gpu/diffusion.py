@@ -6,7 +6,7 @@ solution on return, `kd` the diffusivity per cell (m^2/yr), `dt` the step (yr); 
 iterations. `Workspace` holds the device handle for one raster shape (the reference's `Workspace`
 keeps the solve's vectors, diffusion.rs:214-260), `Dims` the raster (grid.rs:11-17). Only the
 multigrid solver is on the device (`DiffusionSolver::Multigrid`, the surface stage's default);
-`solve_with` exposes the BASELINE variants (red-black cycle, FP64 cycle, mixed precision,
+`solve_with` exposes the benchmark's variants (red-black cycle, FP64 cycle, mixed precision,
 relative-residual rule). Every call goes through the C ABI; nothing here computes on the CPU.
 """
 from __future__ import annotations
@@ -52,6 +52,7 @@ def _declare(lib):
     lib.dt_diff_operator.argtypes = [vp, vp, d, vp, vp]
     lib.dt_diff_vcycle.argtypes = [vp, vp, d, i, vp, vp, ctypes.POINTER(i)]
     lib.dt_diff_lod.argtypes = [vp, vp, vp, d, vp]
+    lib.dt_diff_profile_kernels.argtypes = [vp, vp, d, i, vp, vp]
     lib._diff_declared = True
 
 
@@ -118,6 +119,18 @@ class Workspace:
         L.check(L.lib().dt_diff_vcycle(self._h, _ptr(kd), float(dt), cycle, _ptr(r), ctypes.c_void_p(z.ctypes.data),
                                        ctypes.byref(levels)))
         return z, levels.value
+
+    # the kernels dt_diff_profile_kernels times, in its order
+    PROFILE_KERNELS = ("apply_fp64", "apply_fp32", "rb2_pre_fp32", "rb2_post_fp32", "rb2_pre_fp64", "rb2_post_fp64")
+
+    def profile_kernels(self, kd, dt, reps=20):
+        """{name: (ms a launch, algorithmic bytes a launch)} of the finest level's hot kernels for
+        the operator of kd and dt, each launch timed alone after an L2 flush."""
+        kd = _f64(kd)
+        k = len(self.PROFILE_KERNELS)
+        ms, by = (ctypes.c_double * k)(), (ctypes.c_double * k)()
+        L.check(L.lib().dt_diff_profile_kernels(self._h, _ptr(kd), float(dt), int(reps), ms, by))
+        return {name: (ms[q], by[q]) for q, name in enumerate(self.PROFILE_KERNELS)}
 
 
 def solve(ws: Workspace, d: Dims, h: np.ndarray, kd, dt: float, solver: str = MULTIGRID, tol_m: float = 1e-5) -> int:

@@ -9,8 +9,8 @@ Per step:
             the U-Net's first guess (kept by the preconditioned-residual rule), to relative
             residual 1e-8; rigidity D = 10^(21 + 3u), u smoothed over --sigma cells; load
             2700 g h, h a |k|^-2 field of std 1500 m
-  diffusion FP32 inner CG and red-black Gauss-Seidel V(2,2) cycles inside FP64 refinement, to
-            relative residual 1e-8; h a |k|^-2.5 field of std 800 m, kappa dt / dx^2 log-uniform
+  diffusion one FP32 CG on red-black Gauss-Seidel V(2,2) cycles with FP64 reliable updates (the
+            residual replaced by the FP64 b - A x), to relative residual 1e-8; h a |k|^-2.5 field of std 800 m, kappa dt / dx^2 log-uniform
             over [0.1, 100] smoothed over --sigma cells
 The plain FP64 path (mean-D preconditioner; FP64 CG and cycle) and the FP64 path with the
 reference's preconditioner run --plain-steps steps each on the same seeds. With --cpu, the
@@ -77,7 +77,7 @@ def main():
                        max_iterations=20000)
     bank_f = F.params(precond=L.PRECOND_REFERENCE, stop=L.STOP_REL_RESIDUAL, precision=L.PREC_FP64, tol=args.tol,
                       max_iterations=20000)
-    fast_d = Dm.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_MIXED, stop=L.STOP_REL_RESIDUAL, tol=args.tol, max_iterations=2000)
+    fast_d = Dm.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_MIXED_RELIABLE, stop=L.STOP_REL_RESIDUAL, tol=args.tol, max_iterations=2000)
     plain_d = Dm.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_FP64, stop=L.STOP_REL_RESIDUAL, tol=args.tol, max_iterations=2000)
 
     def fields(step):

@@ -172,12 +172,23 @@ dt_status dt_diff_solve(dt_diff* s, double* h_inout, const double* kd, double dt
 dt_status dt_diff_solve_dev(dt_diff* s, double* h_inout, const double* kd, double dt, const dt_diff_params* p, dt_report* rep);
 /* y = (I + dt L_kd) x (host arrays). */
 dt_status dt_diff_operator(dt_diff* s, const double* kd, double dt, const double* x, double* y);
-/* z = M^-1 r, one V-cycle from z = 0 (FP32 levels), for tests of the cycle; `levels` receives
- * the hierarchy's depth. */
 /* x = the LOD splitting's first guess (diffusion.rs:370-489) from h (host arrays; the solve's own
  * first guess, for tests) */
 dt_status dt_diff_lod(dt_diff* s, const double* h, const double* kd, double dt, double* x);
+/* z = M^-1 r, one V-cycle from z = 0 (FP32 levels), for tests of the cycle; `levels` receives
+ * the hierarchy's depth. */
 dt_status dt_diff_vcycle(dt_diff* s, const double* kd, double dt, int cycle, const double* r, float* z, int* levels);
+/* Benchmark support (no counterpart in the reference): the average device time (ms) of the
+ * finest level's hot kernels for the operator of kd and dt (host array), each launch timed alone
+ * with CUDA events on the handle's stream after a write of a buffer twice the L2, and each
+ * kernel's algorithmic bytes per launch. Kernel ids, DT_DIFF_PROFILE_KERNELS of them: 0 the CG
+ * operator y = A x with x.y in FP64, 1 the same in FP32, 2 the Gauss-Seidel pre-smoothing (two
+ * red-black sweeps from z = 0, the residual's restriction fused) in FP32, 3 the post-smoothing
+ * (the coarse correction fused, two sweeps) in FP32, 4 and 5 those two in FP64. Rasters whose
+ * finest level does not take the tiled sweeps (odd periodic widths, widths under 42) return
+ * DT_UNSUPPORTED. */
+#define DT_DIFF_PROFILE_KERNELS 6
+dt_status dt_diff_profile_kernels(dt_diff* s, const double* kd, double dt, int reps, double* ms, double* bytes);
 
 /* ---- learned warm start ----------------------------------------------------------------------
  * No counterpart in the reference: a 4-level U-Net (32/64/128/256 channels, 3 x 3 convolutions,

@@ -18,7 +18,7 @@
 //
 // Additions that the reference does not have, each labelled where it is defined: the cycle in
 // f64 as well as f32, the red-black Gauss-Seidel V(2,2) cycle to a 16 x 8 coarsest level, and the
-// relative-residual stopping rule of the BASELINE configurations.
+// relative-residual stopping rule of the benchmark's configurations.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -292,7 +292,7 @@ static const int NU = 2;                // multigrid.rs:48
 static const float SCALE = 0.5f;        // multigrid.rs:52
 static const size_t COARSEST = 64;      // multigrid.rs:54
 static const int COARSE_SWEEPS = 16;    // multigrid.rs:56
-// Not in the reference: the BASELINE cycle's coarsest level (16 x 8 cells) and its sweeps.
+// Not in the reference: the benchmark's cycle's coarsest level (16 x 8 cells) and its sweeps.
 static const size_t COARSEST_RB = 128;
 static const int COARSE_SWEEPS_RB = 8;
 
@@ -453,7 +453,7 @@ struct Level {
     }
   }
 
-  // Not in the reference (BASELINE's smoother): the colour of cell (i, j) for the multi-colour
+  // Not in the reference (the benchmark's smoother): the colour of cell (i, j) for the multi-colour
   // Gauss-Seidel sweeps. Red/black is (i + j) % 2; on a wrapping level of odd width the ring of a
   // row is an odd cycle, so its last column takes two colours of its own (2 + j % 2). No two
   // cells of one colour are neighbours, so a colour's cells may be updated in any order (or all
@@ -496,7 +496,7 @@ struct Level {
 template <typename T>
 struct Hierarchy {
   std::vector<Level<T>> levels;
-  int kind;  // DTO_CYCLE_JACOBI (the reference's) or DTO_CYCLE_RBGS (BASELINE's)
+  int kind;  // DTO_CYCLE_JACOBI (the reference's) or DTO_CYCLE_RBGS (the benchmark's)
   T omega, scale;
   int nu;
 
@@ -533,7 +533,7 @@ struct Hierarchy {
     return acc;
   }
 
-  // Not in the reference: BASELINE's symmetric red-black Gauss-Seidel V(nu, nu) cycle from z = 0.
+  // Not in the reference: the benchmark's symmetric red-black Gauss-Seidel V(nu, nu) cycle from z = 0.
   // Pre-smoothing sweeps the colours forward, post-smoothing backward (the adjoint order), so the
   // cycle is a symmetric positive definite operator; the coarsest level takes COARSE_SWEEPS_RB
   // forward sweeps and as many backward ones.

@@ -15,7 +15,7 @@
 // The operation order of each cell's arithmetic follows the reference (no fused multiply-add:
 // built with -ffp-contract=off). Two additions that the reference does not have are labelled:
 // the single-level constant-mean-D preconditioner and the relative-residual stopping rule of the
-// BASELINE configurations.
+// benchmark configurations.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -309,7 +309,7 @@ struct Bank {  // surface/flexure.rs:1352-1402
     return bk;
   }
 
-  // Not in the reference: BASELINE's constant-mean-D preconditioner, one spectral level at the
+  // Not in the reference: the benchmark's constant-mean-D preconditioner, one spectral level at the
   // arithmetic means of d and c (the prototype's method D, docs/design/flexure.md:190).
   static Bank mean(size_t n, const double* dv, const double* c) {
     Bank bk;
@@ -420,7 +420,7 @@ class Solver {  // surface/flexure.rs:1471-1741
     std::vector<double> jacobi, left, part;
   };
 
-  // surface/flexure.rs:1417-1468 (reference) or the single mean level (BASELINE, no sweeps).
+  // surface/flexure.rs:1417-1468 (reference) or the single mean level (the benchmark's plain method, no sweeps).
   Pre make_pre(const double* d, const double* c, int precond) const {
     Pre pre;
     pre.d = d;
@@ -474,7 +474,7 @@ class Solver {  // surface/flexure.rs:1471-1741
     for (long k = 0; k < (long)n; ++k) z[k] += (r[k] - left[k]) * jac[k];
   }
 
-  // surface/flexure.rs:1680-1740, with the BASELINE stopping rule as an option.
+  // surface/flexure.rs:1680-1740, with the benchmark's stopping rule as an option.
   void solve(const double* d, const double* c, const double* b, double* x, double tol, int max_it, int precond, int stop,
              dto_report* rep) {
     Pre pre = make_pre(d, c, precond);

@@ -1,7 +1,7 @@
 """Parity of the device diffusion solve with the CPU oracle, through the C ABI.
 
 Ports of crates/deeptime-core/src/surface/diffusion/multigrid/tests.rs run on the device (same
-sizes, seeds, tolerances and bounds), plus the BASELINE variants against the oracle. The cycle runs
+sizes, seeds, tolerances and bounds), plus the benchmark's variants against the oracle. The cycle runs
 in FP32 (as the reference's), so cycles are compared at 1e-4 of the reference's own symmetric
 tolerance scale, and solves by the reference's error bound.
 """
@@ -198,3 +198,37 @@ def test_the_fused_gauss_seidel_cycle_is_bit_for_bit_the_per_colour_launches(w, 
         xa, ra = apart.solve_with(z0, kd, 2.0e6, p)
         assert rf.iterations == ra.iterations, (precision, rf.iterations, ra.iterations)
         assert np.abs(xf - xa).max() <= 1e-12 * np.abs(xa).max(), (precision, float(np.abs(xf - xa).max()))
+
+
+@pytest.mark.parametrize("w,h,wrap", [(2048, 1024, True), (2050, 1030, False), (2000, 1201, False)])
+def test_the_large_sweep_tiles_are_bit_for_bit_the_small_ones(w, h, wrap, monkeypatch):
+    # k_mg_rb2 on 64 x 32 tiles (FP32 levels of at least four tiles an SM, the default) against
+    # 32 x 16 tiles (DT_MG_BIG_TILES=0 at create), on rasters whose last tiles are ragged: the
+    # same updates in the same order, so the same bits
+    z0 = terrain(w, h, 13)
+    kd = shelf_kd(z0, 13)
+    r = np.random.default_rng(w * h).random((h, w)) - 0.5
+    big = D.Workspace(D.Dims(w, h, 2400.0, wrap))
+    monkeypatch.setenv("DT_MG_BIG_TILES", "0")
+    small = D.Workspace(D.Dims(w, h, 2400.0, wrap))
+    monkeypatch.delenv("DT_MG_BIG_TILES")
+    zb, lb = big.vcycle(kd, 2.0e6, r, L.CYCLE_RBGS)
+    zs, ls = small.vcycle(kd, 2.0e6, r, L.CYCLE_RBGS)
+    assert lb == ls and np.array_equal(zb, zs), float(np.abs(zb - zs).max())
+    p = D.params(cycle=L.CYCLE_RBGS, precision=L.DIFF_MIXED_RELIABLE, stop=L.STOP_REL_RESIDUAL, tol=1e-10, max_iterations=2000)
+    xb, rb = big.solve_with(z0, kd, 2.0e6, p)
+    xs, rs = small.solve_with(z0, kd, 2.0e6, p)
+    assert rb.iterations == rs.iterations and np.array_equal(xb, xs)
+
+
+def test_the_kernel_profile_reports_every_kernel():
+    # dt_diff_profile_kernels on the benchmark's raster: a positive time and the algorithmic bytes
+    w, h = 2048, 1024
+    z0 = terrain(w, h, 17)
+    kd = shelf_kd(z0, 17)
+    ws = D.Workspace(D.Dims(w, h, 10_000.0, True))
+    prof = ws.profile_kernels(kd, 1.0, reps=2)
+    assert list(prof) == list(D.Workspace.PROFILE_KERNELS)
+    n = w * h
+    assert prof["apply_fp64"][1] == 40 * n and prof["apply_fp32"][1] == 20 * n
+    assert all(t > 0 for t, _ in prof.values())

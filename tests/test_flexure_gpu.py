@@ -2,7 +2,7 @@
 
 Tolerances: the operator and transforms are FP64 kernels, compared at 1e-12 relative (different
 operation order and fused multiply-adds, nothing else); converged solves are compared by their
-relative L2 distance, at most 1e-8 (BASELINE's bar) when both are solved well below it.
+relative L2 distance, at most 1e-8 (the benchmark's bar) when both are solved well below it.
 """
 import math
 

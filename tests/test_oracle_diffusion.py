@@ -77,7 +77,7 @@ def test_the_multigrid_and_jacobi_solves_agree_within_their_tolerance():
 
 @pytest.mark.parametrize("cycle", [O.CYCLE_JACOBI, O.CYCLE_RBGS])
 def test_the_cycle_is_a_symmetric_positive_definite_operator(cycle):
-    # multigrid/tests.rs:243-289 (and the same property for BASELINE's red-black cycle)
+    # multigrid/tests.rs:243-289 (and the same property for the benchmark's red-black cycle)
     for w, h, wrap in [(64, 40, True), (37, 23, False), (5, 3, True), (2, 9, True), (1, 1, False), (64, 32, True)]:
         z = terrain(w, h, 5)
         kd = shelf_kd(z, 5)
@@ -105,7 +105,7 @@ def test_the_cycle_takes_far_fewer_iterations_than_jacobi_on_a_shelf():
 
 @pytest.mark.parametrize("precision", [32, 64])
 def test_the_red_black_cycle_solves_to_a_relative_residual(precision):
-    # BASELINE's variant: V(2,2) red-black Gauss-Seidel to 16 x 8, relative residual 1e-10.
+    # the benchmark's variant: V(2,2) red-black Gauss-Seidel to 16 x 8, relative residual 1e-10.
     w, h = 128, 64
     b = terrain(w, h, 4)
     kd = shelf_kd(b, 4)

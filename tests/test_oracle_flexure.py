@@ -287,7 +287,7 @@ def test_the_operator_is_symmetric_and_the_preconditioner_is_spd():
 
 
 def test_the_relative_residual_rule_reaches_its_tolerance():
-    # BASELINE's stopping rule (not the reference's): ||r|| / ||b|| <= tol, both preconditioners.
+    # the benchmark's stopping rule (not the reference's): ||r|| / ||b|| <= tol, both preconditioners.
     w, h, dx = 64, 32, 10_000.0
     rng = np.random.default_rng(3)
     te = patchy(w, h, 8.0, 60.0)
