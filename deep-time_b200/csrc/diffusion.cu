@@ -1017,30 +1017,41 @@ __global__ void __launch_bounds__(128) k_lod_chunks(int L, int n, int P, double 
   }
   double west = s == 0 ? (ROWS ? fw : 0.0) : ln.face(s - 1);
   double bt = 1.0, cprev = 0.0, pv0 = 0.0, pv1 = 0.0, qv = 0.0, rv = 0.0;
+  // the walk's inputs one position ahead (K(i + 1) and the right-hand side), so that their loads
+  // overlap the recurrence; each K read once (face(i) = 0.5 (K(i) + K(i + 1)) dt / dx^2)
+  double kn = ln.K(s), bn = p0[at(s)];
   for (int i = s; i < e; ++i) {
-    const double east = ln.face(i);
+    const double ki = kn, b0 = bn;
+    double east;
+    if (i + 1 < n) {
+      kn = ln.K(i + 1);
+      east = 0.5 * (ki + kn) * dtdx2;
+    } else {
+      east = ROWS ? 0.5 * (ki + ln.K(0)) * dtdx2 : 0.0;
+    }
+    if (i + 1 < e) bn = p0[at(i + 1)];
     double di = 1.0 + west + east;
     if (ROWS && i == 0) di = di - gamma;
     if (ROWS && i == n - 1) di = di - alpha * beta / gamma;
     const double lo = i == 0 ? 0.0 : -west;
     const double up = (ROWS && i == n - 1) ? 0.0 : -east;
-    const double b0 = p0[at(i)];
     const double b1 = ROWS ? (i == 0 ? gamma : (i == n - 1 ? alpha : 0.0)) : 0.0;
     const double rr = i == e - 1 ? -up : 0.0;
+    // one reciprocal a position for the five quotients
+    bt = i == s ? di : di - lo * cprev;
+    const double ib = 1.0 / bt;
     if (i == s) {
-      bt = di;
-      pv0 = b0 / bt;
-      pv1 = b1 / bt;
-      qv = -lo / bt;
-      rv = rr / bt;
+      pv0 = b0 * ib;
+      pv1 = b1 * ib;
+      qv = -lo * ib;
+      rv = rr * ib;
     } else {
-      bt = di - lo * cprev;
-      pv0 = (b0 - lo * pv0) / bt;
-      pv1 = (b1 - lo * pv1) / bt;
-      qv = (0.0 - lo * qv) / bt;
-      rv = (rr - lo * rv) / bt;
+      pv0 = (b0 - lo * pv0) * ib;
+      pv1 = (b1 - lo * pv1) * ib;
+      qv = (0.0 - lo * qv) * ib;
+      rv = (rr - lo * rv) * ib;
     }
-    cprev = up / bt;
+    cprev = up * ib;
     c[at(i)] = cprev;
     p0[at(i)] = pv0;
     if (ROWS) p1[at(i)] = pv1;
@@ -1050,6 +1061,7 @@ __global__ void __launch_bounds__(128) k_lod_chunks(int L, int n, int P, double 
   }
   // back substitution inside the chunk: y_i -= c_i y_(i+1)
   const double e0 = pv0, e1 = pv1, eq = qv, er = rv;  // the last position's values are final
+#pragma unroll 4
   for (int i = e - 2; i >= s; --i) {
     const double ci = c[at(i)];
     pv0 = p0[at(i)] - ci * pv0;
