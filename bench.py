@@ -662,7 +662,10 @@ def main():
     solve_dev(0, methods["mixed_gpu"][0])
     L.check(lib.dt_flex_profile_kernels(sv._h, L.PREC_MIXED, 20, kms, kbytes))
     levels3 = args.precond == "reference"
-    per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: 3, 4: 3, 9: 1} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 4: 1, 5: 1})
+    # the bank's column and weighted forward row passes: three launches an iteration, or one of the
+    # three levels (the profile then reports three levels' bytes)
+    bank = 3 // max(1, round(kbytes[4] / (8 * W * H)))
+    per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: bank, 4: bank, 9: 1} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 4: 1, 5: 1})
     share = {k: kms[k] * cnt for k, cnt in per_it.items()}
     top = max(share, key=share.get)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(

@@ -3786,6 +3786,10 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
       3 * e * n,  // rows forward weighted: left, w in; half out
       7 * e * n,  // rows inverse of the bank: three spectra, three weights in; part out
   };
+  // the bank's column passes and weighted forward row passes as the solve launches them: the
+  // three levels in one launch (each level's bytes again) where it does so
+  const bool bank1 = s->bank_one_launch && !s->any && !s->row_solve;
+  const double bank_levels = bank1 ? 3.0 : 1.0;
   cudaEvent_t a, b;
   DT_CUDA(cudaEventCreate(&a));
   DT_CUDA(cudaEventCreate(&b));
@@ -3799,11 +3803,27 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
         case 1: k_update<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.x, L.r, L.p, L.ap, s->partials, L.S); break;
         case 2: k_direction<T><<<ew_grid(s), 256, 0, st>>>(s->n, L.p, L.z, L.S); break;
         case 3: launch_rows_fwd<T>(s, L, L.r, nullptr, L.half, g, L.S, st); break;
-        case 4: launch_cols<T>(s, L, L.half, g, 0, L.S, st); break;
+        case 4:
+          if (bank1) {
+            cols_fn<T>(ilog2(s->h), LogSeq{}, s->cols_fused)<<<dim3(g.cgrid, 3), g.cthreads, g.csmem, st>>>(
+                s->N, L.half, L.tab.tw_col, L.tab.omega, L.tab.omega2, L.tab.lx, L.tab.ly, (T)(1.0 / (s->dx * s->dx)), L.S, 0);
+            counted();
+          } else {
+            launch_cols<T>(s, L, L.half, g, 0, L.S, st);
+          }
+          break;
         case 5: launch_rows_inv<T>(s, L, INV_STORE_DOT, L.half, L.z, nullptr, L.r, g, L.S, st); break;
         case 6: launch_apply<T>(s, JAC_LEFT, nullptr, L.J, nullptr, L.d, L.c, L.r, L.left, L.S, st); break;
         case 7: launch_apply<T>(s, JAC_FINAL, nullptr, L.J, L.part, L.d, L.c, L.r, L.z, L.S, st); break;
-        case 8: launch_rows_fwd<T>(s, L, L.left, L.wt[0], L.half, g, L.S, st); break;
+        case 8:
+          if (bank1) {
+            rows_fwd_fn<T, true>(ilog2(s->N), LogSeq{})<<<dim3(g.rgrid, 3), g.rthreads, g.rsmem, st>>>(
+                s->w, s->h, L.left, L.wt[0], L.half, L.tab.tw_row, L.tab.post, L.S);
+            counted();
+          } else {
+            launch_rows_fwd<T>(s, L, L.left, L.wt[0], L.half, g, L.S, st);
+          }
+          break;
         case 9: launch_rows_inv<T>(s, L, INV_BANK, L.half, L.part, L.wt[0], nullptr, g, L.S, st); break;
       }
     };
@@ -3823,7 +3843,7 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
       total += t;
     }
     ms[k] = total / reps;
-    bytes[k] = algo[k];
+    bytes[k] = algo[k] * (k == 4 || k == 8 ? bank_levels : 1.0);
   }
   cudaEventDestroy(a);
   cudaEventDestroy(b);

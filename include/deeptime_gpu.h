@@ -222,7 +222,10 @@ dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
  * kernel's algorithmic bytes per launch. Kernel ids, DT_PROFILE_KERNELS of them: 0 operator +
  * p.Ap, 1 x/r update + r.r, 2 direction, 3 rows forward, 4 column DCT-divide-IDCT, 5 rows
  * inverse + r.z, 6 Jacobi left, 7 Jacobi final, 8 rows forward weighted, 9 rows inverse of
- * the bank (its three levels' weighted sum). `precision` selects the FP64 or the FP32 lane. */
+ * the bank (its three levels' weighted sum). Kernels 4 and 8 are timed as the bank's solve
+ * launches them: where it takes the three levels in one launch (power-of-two transforms), one
+ * launch of the three levels, with three levels' bytes. `precision` selects the FP64 or the FP32
+ * lane. */
 #define DT_PROFILE_KERNELS 10
 dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes);
 
