@@ -79,7 +79,7 @@ def workload_config(n_inputs):
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--inputs", type=int, default=4, help="distinct seeded input sets cycled over the steps")
@@ -185,7 +185,9 @@ def max_over_ranks(v, world):
 
 
 class Clocks:
-    """nvidia-smi samples (200 ms) during the timed region."""
+    """nvidia-smi samples (every 100 ms), started before the warm-up solves and stopped after the
+    timed region; `wait_first` holds until the first sample has arrived, so the sampler is running
+    when the timing starts."""
 
     def __init__(self, index):
         self.index = index
@@ -198,7 +200,7 @@ class Clocks:
              "clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
         except OSError:
@@ -210,6 +212,11 @@ class Clocks:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 8:
                 self.samples.append(parts)
+
+    def wait_first(self, timeout=5.0):
+        t0 = time.perf_counter()
+        while self.proc and not self.samples and time.perf_counter() - t0 < timeout:
+            time.sleep(0.01)
 
     def __exit__(self, *a):
         if self.proc:
@@ -612,9 +619,10 @@ def main():
         barrier(world)
         return e0.elapsed_time(e1), reps
 
-    for i in range(args.warmup):
-        solve_dev(i, head)
     with Clocks(local) as clk:
+        for i in range(args.warmup):
+            solve_dev(i, head)
+        clk.wait_first()
         ms, reps = timed(lambda i: solve_dev(i, head), args.steps)
     ms = max_over_ranks(ms, world)
     its = [r.iterations for r in reps]

@@ -189,9 +189,9 @@ __global__ void __launch_bounds__(256) k_d_apply(int w, int h, int wrap, const T
   acc.v[0] = 0.0;
   acc.v[1] = 0.0;
   constexpr int V = 16 / sizeof(T);
-  if (w % V == 0 && d_aligned16(east) && d_aligned16(south) && d_aligned16(diag) && d_aligned16(x) && d_aligned16(b) &&
-      d_aligned16(y)) {
-    // whole rows of 16-byte chunks: each thread a chunk at a time
+  if (w % V == 0 && n < ((size_t)1 << 31) && d_aligned16(east) && d_aligned16(south) && d_aligned16(diag) && d_aligned16(x) &&
+      d_aligned16(b) && d_aligned16(y)) {
+    // whole rows of 16-byte chunks, fewer than 2^31 cells: each thread a chunk at a time
     const unsigned int chunks = (unsigned int)(w / V), nch = chunks * (unsigned int)h;
     for (unsigned int q = blockIdx.x * blockDim.x + threadIdx.x; q < nch; q += gridDim.x * blockDim.x) {
       const int j = (int)(q / chunks), i0 = (int)(q - (unsigned int)j * chunks) * V;
