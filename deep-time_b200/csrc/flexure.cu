@@ -3002,7 +3002,7 @@ __global__ void k_add_to64(size_t n, double* __restrict__ x, const T* __restrict
 __global__ void k_keep_rz(const Scalars* S, double* slot) { *slot = S->rz; }
 
 // Keep x0 when its preconditioned residual is below the zero guess's, r0.M^-1 r0 < b.M^-1 b;
-// otherwise x = 0, r = b. The 2-norm of the residual cannot judge a predicted guess: the
+// otherwise x = 0, r = b. The 2-norm of the residual cannot rate a predicted guess: the
 // operator multiplies the prediction's grid-scale rounding noise by up to d lambda^2 / c
 // (1e5 to 1e8 on these rasters), while M^-1 weighs the residual as the error's energy does.
 __global__ void k_warm_decide_pre(size_t n, double* __restrict__ x, double* __restrict__ r, const double* __restrict__ b,
