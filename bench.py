@@ -55,7 +55,7 @@ W, H, DX, SIGMA = 4096, 2048, 2500.0, 32.0
 TOL = 1e-8
 REF_THREADS = 8  # the reference's own benchmark runs its solver pool on 8 threads
 KERNEL_NAMES = ["flex_apply", "cg_update", "cg_direction", "fft_rows_fwd", "dct_cols_divide_idct", "fft_rows_inv_dot",
-                "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_bank"]
+                "jacobi_left", "jacobi_final", "fft_rows_fwd_weighted", "fft_rows_inv_bank", "dct_cols_divide_idct_one_level"]
 WEIGHTS = os.path.join(ROOT, "deep-time_b200", "weights", "unet_flexure.bin")
 MODEL_DX = 10_000.0  # the U-Net's cell size: trained on 512 x 256 rasters of 10 km
 METRIC = "flexure solves/s to relative residual 1e-8 @4096x2048 (time-to-1e-8 per solve = 1000/value ms)"
@@ -665,15 +665,16 @@ def main():
     ems = max_over_ranks(ems, world)
 
     # per-kernel launch durations (events) for the roofline
-    kms = (ctypes.c_double * 10)()
-    kbytes = (ctypes.c_double * 10)()
+    kms = (ctypes.c_double * len(KERNEL_NAMES))()
+    kbytes = (ctypes.c_double * len(KERNEL_NAMES))()
     solve_dev(0, methods["mixed_gpu"][0])
     L.check(lib.dt_flex_profile_kernels(sv._h, L.PREC_MIXED, 20, kms, kbytes))
     levels3 = args.precond == "reference"
     # the bank's column and weighted forward row passes: three launches an iteration, or one of the
-    # three levels (the profile then reports three levels' bytes)
-    bank = 3 // max(1, round(kbytes[4] / (8 * W * H)))
-    per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: bank, 4: bank, 9: 1} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 4: 1, 5: 1})
+    # three levels (the profile then reports three levels' bytes: 8 bytes a cell a level in the
+    # FP32 lane); the mean-D preconditioner's one column pass is kernel 10
+    bank = 3 // max(1, round(kbytes[4] / (2 * 4 * W * H)))
+    per_it = ({0: 1, 1: 1, 2: 1, 6: 1, 7: 1, 8: bank, 4: bank, 9: 1} if levels3 else {0: 1, 1: 1, 2: 1, 3: 1, 10: 1, 5: 1})
     share = {k: kms[k] * cnt for k, cnt in per_it.items()}
     top = max(share, key=share.get)
     peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(

@@ -3785,6 +3785,7 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
       6 * e * n,  // Jacobi final: r, J, part, d, c in; z out
       3 * e * n,  // rows forward weighted: left, w in; half out
       7 * e * n,  // rows inverse of the bank: three spectra, three weights in; part out
+      2 * e * n,  // columns of one level (the constant-mean-D preconditioner's pass)
   };
   // the bank's column passes and weighted forward row passes as the solve launches them: the
   // three levels in one launch (each level's bytes again) where it does so
@@ -3825,6 +3826,7 @@ static dt_status profile_lane(dt_flex* s, Lane<T>& L, int reps, double* ms, doub
           }
           break;
         case 9: launch_rows_inv<T>(s, L, INV_BANK, L.half, L.part, L.wt[0], nullptr, g, L.S, st); break;
+        case 10: launch_cols<T>(s, L, L.half, g, 0, L.S, st); break;
       }
     };
     one();  // warm

@@ -224,9 +224,9 @@ dt_status dt_flex_set_unet(dt_flex* s, dt_unet* u, double model_dx);
  * inverse + r.z, 6 Jacobi left, 7 Jacobi final, 8 rows forward weighted, 9 rows inverse of
  * the bank (its three levels' weighted sum). Kernels 4 and 8 are timed as the bank's solve
  * launches them: where it takes the three levels in one launch (power-of-two transforms), one
- * launch of the three levels, with three levels' bytes. `precision` selects the FP64 or the FP32
- * lane. */
-#define DT_PROFILE_KERNELS 10
+ * launch of the three levels, with three levels' bytes; 10 is the column pass of one level, the
+ * constant-mean-D preconditioner's. `precision` selects the FP64 or the FP32 lane. */
+#define DT_PROFILE_KERNELS 11
 dt_status dt_flex_profile_kernels(dt_flex* s, int precision, int reps, double* ms, double* bytes);
 
 /* Implicit diffusion on the cube grid (surface/cube/diffusion.rs::solve with
